@@ -1,0 +1,318 @@
+"""gzippy_b200 -- B200 (sm_100a) gzip decompression behind gzippy's API.
+
+Mirrors the reference's public decode API (JackDanger/gzippy v0.8.0,
+src/lib.rs:176-227):
+
+    decompress(data) -> bytes
+    decompress_with_threads(data, threads) -> bytes
+    decompress_to_writer(data, writer) -> int
+    decompress_to_writer_with_threads(data, writer, threads) -> int
+
+Non-gzip input returns b"" / 0 (src/lib.rs:50-52).  Corrupt or truncated
+input raises GzippyError (kind "Decompression", src/error.rs:7-46).  The
+thread count of the reference has no meaning on the device; it is accepted
+and ignored.  Every call goes through the C ABI of libgzgpu.so
+(include/gzgpu.h); there is no CPU fallback: without the CUDA library or a
+CUDA device the calls raise.
+
+Beyond the reference: decompress_batch (many streams per launch) and
+Server (continuous-batching request loop).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+
+import numpy as np
+
+from . import build as _build
+
+__all__ = ["GzippyError", "decompress", "decompress_with_threads", "decompress_to_writer",
+           "decompress_to_writer_with_threads", "decompress_batch", "Context", "Stats", "lib"]
+
+OK, NOT_GZIP, BAD_HEADER, BAD_DEFLATE, CRC_MISMATCH, SIZE_MISMATCH, OUT_TOO_SMALL = range(7)
+DEVICE_ERROR, TIMEOUT, TRUNCATED, INVALID_ARGUMENT = 7, 8, 9, 12
+
+
+class GzippyError(Exception):
+    """gzippy's GzippyError; `kind` is the variant name, `code` the C status."""
+
+    def __init__(self, kind: str, message: str, code: int = 0):
+        super().__init__(f"{kind} error: {message}")
+        self.kind = kind
+        self.code = code
+
+
+class Config(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int), ("chunk_bytes", ctypes.c_size_t),
+                ("lut_bits", ctypes.c_int), ("autotune", ctypes.c_int)]
+
+
+class Span(ctypes.Structure):
+    _fields_ = [("data", ctypes.c_void_p), ("len", ctypes.c_size_t)]
+
+
+class Out(ctypes.Structure):
+    _fields_ = [("data", ctypes.c_void_p), ("cap", ctypes.c_size_t), ("len", ctypes.c_size_t)]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = ([(n, ctypes.c_double) for n in
+                 ("ms_total", "ms_h2d", "ms_scan", "ms_find", "ms_decode", "ms_walk",
+                  "ms_resolve", "ms_crc", "ms_d2h", "ms_decode_kernel")] +
+                [(n, ctypes.c_uint64) for n in
+                 ("in_bytes", "out_bytes", "n_streams", "n_members", "n_chunks", "n_accepted",
+                  "n_rejected", "n_repairs", "n_tail_marker_chunks", "n_pages", "decode_passes",
+                  "kernel_launches", "chunk_bytes")] +
+                [("lut_bits", ctypes.c_int32), ("pad", ctypes.c_int32)])
+
+    def as_dict(self) -> dict:
+        return {n: getattr(self, n) for n, _ in self._fields_ if n != "pad"}
+
+
+WRITE_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t)
+
+_lock = threading.Lock()
+_lib = None
+_default_ctx = None
+
+
+def lib():
+    """The loaded libgzgpu.so (built in-tree on first use if missing)."""
+    global _lib
+    with _lock:
+        if _lib is None:
+            path = _build.LIB
+            if not os.path.exists(path):
+                _build.build()
+            L = ctypes.CDLL(path)
+            vp, sz = ctypes.c_void_p, ctypes.c_size_t
+            L.gzgpu_create.argtypes = [ctypes.POINTER(vp), ctypes.POINTER(Config)]
+            L.gzgpu_destroy.argtypes = [vp]
+            L.gzgpu_strerror.argtypes = [ctypes.c_int]
+            L.gzgpu_strerror.restype = ctypes.c_char_p
+            L.gzgpu_decompress.argtypes = [vp, vp, sz, vp, sz, ctypes.POINTER(sz)]
+            L.gzgpu_decompress_device.argtypes = [vp, vp, sz, vp, sz, ctypes.POINTER(sz)]
+            L.gzgpu_decompress_to_writer.argtypes = [vp, vp, sz, WRITE_FN, vp,
+                                                     ctypes.POINTER(ctypes.c_uint64)]
+            L.gzgpu_decompress_batch.argtypes = [vp, ctypes.POINTER(Span), sz, ctypes.POINTER(Out),
+                                                 ctypes.POINTER(ctypes.c_int)]
+            L.gzgpu_get_stats.argtypes = [vp, ctypes.POINTER(Stats)]
+            L.gzgpu_debug_find.argtypes = [vp, vp, sz, vp, vp, sz, vp, vp, vp]
+            L.gzgpu_debug_decode.argtypes = [vp, vp, sz, vp, vp, vp, sz, vp, sz, vp]
+            _lib = L
+    return _lib
+
+
+def strerror(code: int) -> str:
+    return lib().gzgpu_strerror(code).decode()
+
+
+def _raise(code: int):
+    if code == TRUNCATED:
+        raise GzippyError("Decompression", strerror(code), code)
+    if code == INVALID_ARGUMENT:
+        raise GzippyError("InvalidArgument", strerror(code), code)
+    raise GzippyError("Decompression", strerror(code), code)
+
+
+def _as_u8(data) -> np.ndarray:
+    if isinstance(data, np.ndarray):
+        return np.ascontiguousarray(data.reshape(-1).view(np.uint8))
+    return np.frombuffer(memoryview(data).cast("B"), dtype=np.uint8)
+
+
+class Context:
+    """One device context (gzgpu_ctx): device buffers, stream, statistics."""
+
+    def __init__(self, device: int = 0, chunk_bytes: int = 0, lut_bits: int = 0,
+                 autotune: bool = False):
+        self._lib = lib()
+        cfg = Config(device, chunk_bytes, lut_bits, int(autotune))
+        h = ctypes.c_void_p()
+        rc = self._lib.gzgpu_create(ctypes.byref(h), ctypes.byref(cfg))
+        if rc != OK:
+            raise GzippyError("Internal", f"gzgpu_create: {strerror(rc)}", rc)
+        self._h = h
+        self._hint = 0
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.gzgpu_destroy(self._h)
+            self._h = None
+
+    def __del__(self):  # pragma: no cover
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def stats(self) -> Stats:
+        s = Stats()
+        self._lib.gzgpu_get_stats(self._h, ctypes.byref(s))
+        return s
+
+    def decompress_into(self, data, out: np.ndarray) -> int:
+        """Decode into a caller buffer; returns bytes written; raises on error."""
+        a = _as_u8(data)
+        n = ctypes.c_size_t(0)
+        rc = self._lib.gzgpu_decompress(self._h, a.ctypes.data, a.size, out.ctypes.data,
+                                        out.size, ctypes.byref(n))
+        if rc == NOT_GZIP:
+            return 0
+        if rc != OK:
+            if rc == OUT_TOO_SMALL:
+                raise GzippyError("Decompression", f"output needs {n.value} bytes", rc)
+            _raise(rc)
+        return n.value
+
+    def decompress(self, data) -> bytes:
+        a = _as_u8(data)
+        cap = max(self._hint, a.size * 4 + 4096)
+        for _ in range(3):
+            out = np.empty(cap, dtype=np.uint8)
+            n = ctypes.c_size_t(0)
+            rc = self._lib.gzgpu_decompress(self._h, a.ctypes.data, a.size, out.ctypes.data, cap,
+                                            ctypes.byref(n))
+            if rc == NOT_GZIP:
+                return b""
+            if rc == OUT_TOO_SMALL:
+                cap = n.value
+                continue
+            if rc != OK:
+                _raise(rc)
+            return out[:n.value].tobytes()
+        _raise(OUT_TOO_SMALL)
+
+    def decompress_to_writer(self, data, writer) -> int:
+        a = _as_u8(data)
+        err = []
+
+        def cb(_user, ptr, n):
+            try:
+                writer.write(ctypes.string_at(ptr, n))
+                return 0
+            except Exception as e:  # pragma: no cover
+                err.append(e)
+                return 1
+
+        fn = WRITE_FN(cb)
+        written = ctypes.c_uint64(0)
+        rc = self._lib.gzgpu_decompress_to_writer(self._h, a.ctypes.data, a.size, fn, None,
+                                                  ctypes.byref(written))
+        if err:
+            raise GzippyError("Io", str(err[0]))
+        if rc == NOT_GZIP:
+            return 0
+        if rc != OK:
+            _raise(rc)
+        return written.value
+
+    def decompress_device(self, d_in: int, in_len: int, d_out: int, out_cap: int) -> int:
+        """Device-resident decode (raw device pointers); returns bytes written."""
+        n = ctypes.c_size_t(0)
+        rc = self._lib.gzgpu_decompress_device(self._h, d_in, in_len, d_out, out_cap,
+                                               ctypes.byref(n))
+        if rc == NOT_GZIP:
+            return 0
+        if rc != OK:
+            if rc == OUT_TOO_SMALL:
+                raise GzippyError("Decompression", f"output needs {n.value} bytes", rc)
+            _raise(rc)
+        return n.value
+
+    def debug_find(self, data, ranges):
+        """Finder kernel on explicit bit ranges -> list of (lo, hi) or None."""
+        a = _as_u8(data)
+        n = len(ranges)
+        fr = np.array([r[0] for r in ranges], np.uint64)
+        to = np.array([r[1] for r in ranges], np.uint64)
+        lo = np.zeros(n, np.uint64)
+        hi = np.zeros(n, np.uint64)
+        va = np.zeros(n, np.int32)
+        rc = self._lib.gzgpu_debug_find(self._h, a.ctypes.data, a.size, fr.ctypes.data,
+                                        to.ctypes.data, n, lo.ctypes.data, hi.ctypes.data,
+                                        va.ctypes.data)
+        if rc != OK:
+            _raise(rc)
+        return [(int(lo[i]), int(hi[i])) if va[i] else None for i in range(n)]
+
+    def debug_decode(self, data, chunks, cap_per):
+        """Inflate kernel on explicit chunks [(start_bit, stop_bit, member_first)].
+        Returns (results n x 6 uint64, entries n x cap_per uint16)."""
+        a = _as_u8(data)
+        n = len(chunks)
+        st = np.array([c[0] for c in chunks], np.uint64)
+        sp = np.array([c[1] for c in chunks], np.uint64)
+        mf = np.array([int(c[2]) for c in chunks], np.int32)
+        ent = np.zeros((n, cap_per), np.uint16)
+        res = np.zeros((n, 6), np.uint64)
+        rc = self._lib.gzgpu_debug_decode(self._h, a.ctypes.data, a.size, st.ctypes.data,
+                                          sp.ctypes.data, mf.ctypes.data, n, ent.ctypes.data,
+                                          cap_per, res.ctypes.data)
+        if rc != OK:
+            _raise(rc)
+        return res, ent
+
+    def decompress_batch(self, datas, caps=None):
+        """Decode many streams in one job.  Returns a list of bytes (or a
+        GzippyError instance per failed stream)."""
+        arrs = [_as_u8(d) for d in datas]
+        n = len(arrs)
+        caps = caps or [max(a.size * 8 + 4096, 1 << 16) for a in arrs]
+        for _ in range(3):
+            outs_np = [np.empty(c, dtype=np.uint8) for c in caps]
+            spans = (Span * max(n, 1))()
+            outs = (Out * max(n, 1))()
+            for i, (a, o) in enumerate(zip(arrs, outs_np)):
+                spans[i] = Span(a.ctypes.data, a.size)
+                outs[i] = Out(o.ctypes.data, o.size, 0)
+            st = (ctypes.c_int * max(n, 1))()
+            self._lib.gzgpu_decompress_batch(self._h, spans, n, outs, st)
+            retry = [i for i in range(n) if st[i] == OUT_TOO_SMALL]
+            if retry:
+                caps = [outs[i].len if st[i] == OUT_TOO_SMALL else caps[i] for i in range(n)]
+                continue
+            res = []
+            for i in range(n):
+                if st[i] == OK:
+                    res.append(outs_np[i][:outs[i].len].tobytes())
+                elif st[i] == NOT_GZIP:
+                    res.append(b"")
+                else:
+                    res.append(GzippyError("Decompression", strerror(st[i]), st[i]))
+            return res
+        raise GzippyError("Decompression", "output sizing failed")
+
+
+def _ctx() -> Context:
+    global _default_ctx
+    if _default_ctx is None:
+        _default_ctx = Context()
+    return _default_ctx
+
+
+def decompress(data) -> bytes:
+    """gzippy::decompress (src/lib.rs:176)."""
+    return _ctx().decompress(data)
+
+
+def decompress_with_threads(data, threads: int) -> bytes:
+    """gzippy::decompress_with_threads (src/lib.rs:189)."""
+    return _ctx().decompress(data)
+
+
+def decompress_to_writer(data, writer) -> int:
+    """gzippy::decompress_to_writer (src/lib.rs:204)."""
+    return _ctx().decompress_to_writer(data, writer)
+
+
+def decompress_to_writer_with_threads(data, writer, threads: int) -> int:
+    """gzippy::decompress_to_writer_with_threads (src/lib.rs:221)."""
+    return _ctx().decompress_to_writer(data, writer)
+
+
+def decompress_batch(datas) -> list:
+    """Many independent streams in one job (no reference counterpart)."""
+    return _ctx().decompress_batch(datas)

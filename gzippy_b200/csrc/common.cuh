@@ -1,0 +1,92 @@
+// common.cuh -- device/host shared definitions for the gzip decode kernels.
+//
+// Data layout in HBM (one decode job = one stream, a batch of streams, or a
+// serving tick):
+//   input    : every stream's gzip bytes back to back, + kInputPad zero bytes
+//   chunks   : ChunkDesc[] (what to decode) and ChunkResult[] (what came out)
+//   pages    : PagePool, fixed pages of kPageEntries u16 entries; a chunk's
+//              decoded entries (bytes < 256, window markers >= 32768) live in
+//              the pages it allocated, in allocation order
+//   output   : final bytes, one contiguous range per stream
+#pragma once
+#include <cstdint>
+
+namespace gzgpu {
+
+constexpr uint32_t kWindow = 32768;          // deflate window (entries)
+constexpr uint32_t kRingMask = kWindow - 1;  // decoder history ring = one window
+constexpr uint32_t kMarkerBase = 32768;      // entry >= kMarkerBase: window index + 32768
+constexpr uint32_t kPageEntries = 65536;     // u16 entries per output page
+constexpr uint32_t kFlush = 8192;            // ring -> page flush unit (entries)
+constexpr uint32_t kInputPad = 1024;         // zero bytes after the input buffer
+constexpr uint64_t kNoStop = ~0ull;
+constexpr uint32_t kNoPage = 0xFFFFFFFFu;
+
+// status codes (same numbering as include/gzgpu.h)
+enum : int32_t {
+  kOk = 0,
+  kNotGzip = 1,
+  kBadHeader = 2,
+  kBadDeflate = 3,
+  kCrcMismatch = 4,
+  kSizeMismatch = 5,
+  kOutTooSmall = 6,
+  kDeviceError = 7,
+  kTimeout = 8,
+  kTruncated = 9,
+  kPoolExhausted = 10,
+  kNotDecoded = 11,
+};
+
+enum : uint32_t {
+  kChunkMemberFirst = 1u,  // starts a member: zero window, never emits markers
+  kChunkValid = 2u,        // has a start (member start or a finder candidate)
+};
+
+struct ChunkDesc {
+  uint64_t start_bit;  // absolute bit offset in the input buffer to decode from
+  uint64_t lo_bit;     // earliest acceptable start (stored-block padding), <= start_bit
+  uint64_t stop_lo;    // stop at the first block boundary >= stop_lo
+  uint64_t guess_bit;  // partition start the finder searched from
+  uint64_t limit_bit;  // end of the finder's search range
+  uint64_t in_end;     // byte end of this chunk's stream in the input buffer
+  uint32_t flags;
+  uint32_t stream;     // stream id
+};
+
+struct ChunkResult {
+  uint64_t end_bit;     // bit where decoding stopped
+  uint64_t out_len;     // entries produced
+  uint64_t marker_end;  // 1 + last marker position (0 = no markers)
+  uint32_t last_page;
+  uint32_t prev_page;
+  uint32_t n_pages;
+  uint32_t n_blocks;
+  int32_t status;
+  int32_t final_block;
+};
+
+struct PagePool {
+  uint16_t* data;    // cap * kPageEntries entries
+  uint32_t* owner;   // chunk id per page
+  uint32_t* seq;     // page index within its chunk
+  uint32_t* next;    // allocation counter
+  uint32_t cap;
+};
+
+// resolve plan entry: one accepted chunk in output order
+struct PlacedChunk {
+  uint64_t out_off;      // final output offset of entry 0
+  uint64_t member_off;   // final output offset where the chunk's member begins
+  uint32_t chunk;        // chunk id
+  uint32_t pad;
+};
+
+// CRC block: a run of final output bytes inside one member
+struct CrcBlock {
+  uint64_t off;
+  uint32_t len;
+  uint32_t member;
+};
+
+}  // namespace gzgpu

@@ -1,0 +1,1085 @@
+// engine.cu -- host driver of the B200 gzip decode pipeline and the C ABI.
+//
+// One job decodes a set of streams that sit back to back in one device
+// input buffer.  Stages (device unless noted):
+//   1. stream headers + member scan            (members.cu)
+//   2. chunk grid per member                   (host: partitions of chunk_bytes)
+//   3. block finder + link                     (finder.cu)
+//   4. persistent inflate over the work list   (inflate.cu)
+//   5. chain walk                              (host: accept / repair, as the
+//      reference's consumer_loop, chunk_fetcher.rs:855; repairs re-enter 4)
+//   6. tails, window chain, bodies, CRC        (resolve.cu)
+// The plain path (gzgpu_decompress) runs one stream per job; the batched
+// path runs all of a batch's streams in one job, so every stage is one launch
+// for the whole batch.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <vector>
+
+#include "../../include/gzgpu.h"
+#include "common.cuh"
+#include "finder.cuh"
+#include "inflate.cuh"
+#include "members.cuh"
+#include "resolve.cuh"
+
+using namespace gzgpu;
+
+namespace {
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t cap = 0;
+  cudaError_t ensure(size_t n) {
+    if (n <= cap) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    size_t want = n + n / 4 + 4096;
+    cudaError_t e = cudaMalloc(&p, want);
+    if (e == cudaSuccess) cap = want;
+    return e;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+  }
+  template <typename T>
+  T* as() const {
+    return reinterpret_cast<T*>(p);
+  }
+};
+
+struct HostPinned {
+  void* p = nullptr;
+  size_t cap = 0;
+  bool ensure(size_t n) {
+    if (n <= cap) return true;
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    cap = 0;
+    size_t want = n + n / 4 + 4096;
+    if (cudaMallocHost(&p, want) != cudaSuccess) return false;
+    cap = want;
+    return true;
+  }
+  void release() {
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    cap = 0;
+  }
+};
+
+struct StreamSpec {
+  uint64_t off, len;  // byte range in the device input buffer
+};
+
+struct StreamOut {
+  int status = kOk;
+  uint64_t out_off = 0, out_len = 0;
+};
+
+struct MemberPlan {
+  uint32_t order_begin, order_end;  // range in the stream's chunk order
+  uint64_t trailer;                 // absolute input byte of the CRC32/ISIZE trailer
+  uint64_t out_len;
+};
+
+// per-stream chain walk state (host)
+struct Walker {
+  uint32_t stream;
+  uint32_t c0, c1;          // this stream's grid chunk ids [c0, c1)
+  uint32_t j;               // next grid chunk to consider
+  uint64_t mpos;            // next member header, relative to the stream
+  uint32_t member = 0;
+  int32_t cur = -1;         // chunk being walked
+  bool done = false;
+  int status = kOk;
+  std::vector<uint32_t> order;
+  std::vector<MemberPlan> members;
+  uint32_t member_order_begin = 0;
+  int32_t pending = -1;     // repair chunk id awaiting decode
+};
+
+const char* kErrStr[] = {"ok",
+                         "not a gzip stream",
+                         "invalid gzip header",
+                         "invalid deflate data",
+                         "CRC32 mismatch",
+                         "ISIZE mismatch",
+                         "output buffer too small",
+                         "CUDA device error",
+                         "timed out",
+                         "truncated input",
+                         "device page pool exhausted",
+                         "chunk not decoded",
+                         "invalid argument"};
+
+}  // namespace
+
+struct gzgpu_ctx {
+  std::mutex mu;
+  int dev = 0, sms = 148;
+  cudaStream_t st = nullptr;
+  size_t chunk_bytes = 0;
+  int lut_bits = 10;
+  bool autotune = false;
+  int decode_blocks = 0;
+  cudaEvent_t ev[12];
+  gzgpu_stats stats{};
+  bool crc_ready = false;
+
+  DevBuf in, out, s_off, s_len, info, units, cands, counters, descs, results, spec, work;
+  DevBuf pages, owner, seq, placed, placed_of, list, segs, cblocks, bcrcs, mblk, mtrail, mlen,
+      mcrc, mstatus;
+  HostPinned h_stage;
+  const uint8_t* cur_in = nullptr;  // input buffer of the running job
+  uint8_t* user_out = nullptr;       // caller device output (device-resident API)
+  size_t user_cap = 0;
+  uint8_t* cur_out = nullptr;        // output buffer the job resolved into
+
+  int check(cudaError_t e) {
+    if (e != cudaSuccess) {
+      fprintf(stderr, "gzgpu: CUDA error %s\n", cudaGetErrorString(e));
+      return kDeviceError;
+    }
+    return kOk;
+  }
+
+  cudaError_t launch_decode(uint32_t* d_work_count) {
+    PagePool pool{pages.as<uint16_t>(), owner.as<uint32_t>(), seq.as<uint32_t>(),
+                  counters.as<uint32_t>() + 2, (uint32_t)(pages.cap / (kPageEntries * 2))};
+    pool.cap = (uint32_t)std::min<uint64_t>(pool.cap, std::min(owner.cap, seq.cap) / 4);
+    cudaError_t e = cudaMemsetAsync(counters.as<uint32_t>() + 3, 0, 4, st);
+    if (e != cudaSuccess) return e;
+    stats.kernel_launches++;
+    stats.decode_passes++;
+    switch (lut_bits) {
+      case 11:
+        return launch_inflate<11>(cur_in, descs.as<ChunkDesc>(), results.as<ChunkResult>(),
+                                  work.as<uint32_t>(), d_work_count, counters.as<uint32_t>() + 3,
+                                  pool, decode_blocks, st);
+      case 12:
+        return launch_inflate<12>(cur_in, descs.as<ChunkDesc>(), results.as<ChunkResult>(),
+                                  work.as<uint32_t>(), d_work_count, counters.as<uint32_t>() + 3,
+                                  pool, decode_blocks, st);
+      default:
+        return launch_inflate<10>(cur_in, descs.as<ChunkDesc>(), results.as<ChunkResult>(),
+                                  work.as<uint32_t>(), d_work_count, counters.as<uint32_t>() + 3,
+                                  pool, decode_blocks, st);
+    }
+  }
+
+  int setup_decode_grid() {
+    int per_sm = 1;
+    switch (lut_bits) {
+      case 11: per_sm = inflate_blocks_per_sm<11>(); break;
+      case 12: per_sm = inflate_blocks_per_sm<12>(); break;
+      default: per_sm = inflate_blocks_per_sm<10>(); break;
+    }
+    if (per_sm < 1) per_sm = 1;
+    decode_blocks = per_sm * sms;
+    return kOk;
+  }
+
+  int run(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R);
+};
+
+static uint64_t pick_chunk_bytes(uint64_t in_len) {
+  // enough chunks to fill every decoder slot several times over, but large
+  // enough that block-finder and marker overhead stay small
+  uint64_t c = 128 << 10;
+  if (in_len < (64ull << 20)) c = 64 << 10;
+  if (in_len < (4ull << 20)) c = 32 << 10;
+  return c;
+}
+
+int gzgpu_ctx::run(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R) {
+  const uint32_t ns = (uint32_t)S.size();
+  R.assign(ns, StreamOut{});
+  int rc;
+  auto t_host0 = std::chrono::steady_clock::now();
+  cudaEventRecord(ev[1], st);
+  // ---- 1. stream headers + member scan --------------------------------
+  std::vector<uint64_t> h_off(ns), h_len(ns);
+  uint64_t total_in = 0;
+  for (uint32_t s = 0; s < ns; s++) {
+    h_off[s] = S[s].off;
+    h_len[s] = S[s].len;
+    total_in += S[s].len;
+  }
+  std::vector<ScanUnit> units;
+  const uint64_t kUnit = 1 << 20;
+  for (uint32_t s = 0; s < ns; s++)
+    for (uint64_t b = 0; b < S[s].len; b += kUnit)
+      units.push_back(ScanUnit{s, 0, b, std::min(S[s].len, b + kUnit)});
+  if ((rc = check(s_off.ensure(8 * ns))) || (rc = check(s_len.ensure(8 * ns))) ||
+      (rc = check(info.ensure(sizeof(StreamInfo) * ns))) ||
+      (rc = check(units.empty() ? cudaSuccess : this->units.ensure(sizeof(ScanUnit) * units.size()))) ||
+      (rc = check(counters.ensure(64))))
+    return rc;
+  uint32_t cand_cap = (uint32_t)std::min<uint64_t>(total_in / 4096 + 4096, 1u << 22);
+  if ((rc = check(cands.ensure(sizeof(MemberCand) * cand_cap)))) return rc;
+  cudaMemcpyAsync(s_off.p, h_off.data(), 8 * ns, cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(s_len.p, h_len.data(), 8 * ns, cudaMemcpyHostToDevice, st);
+  if (!units.empty())
+    cudaMemcpyAsync(this->units.p, units.data(), sizeof(ScanUnit) * units.size(),
+                    cudaMemcpyHostToDevice, st);
+  cudaMemsetAsync(counters.p, 0, 64, st);
+  if ((rc = check(launch_stream_headers(cur_in, s_off.as<uint64_t>(), s_len.as<uint64_t>(),
+                                        ns, info.as<StreamInfo>(), st))))
+    return rc;
+  if ((rc = check(launch_member_scan(cur_in, this->units.as<ScanUnit>(),
+                                     (uint32_t)units.size(), s_off.as<uint64_t>(),
+                                     s_len.as<uint64_t>(), info.as<StreamInfo>(),
+                                     cands.as<MemberCand>(), counters.as<uint32_t>(), cand_cap, sms,
+                                     st))))
+    return rc;
+  stats.kernel_launches += 2;
+  std::vector<StreamInfo> hinfo(ns);
+  uint32_t n_cand = 0;
+  cudaMemcpyAsync(hinfo.data(), info.p, sizeof(StreamInfo) * ns, cudaMemcpyDeviceToHost, st);
+  cudaMemcpyAsync(&n_cand, counters.p, 4, cudaMemcpyDeviceToHost, st);
+  if ((rc = check(cudaStreamSynchronize(st)))) return rc;
+  cudaEventRecord(ev[2], st);
+  n_cand = std::min(n_cand, cand_cap);
+  std::vector<MemberCand> hc(n_cand);
+  if (n_cand) {
+    cudaMemcpyAsync(hc.data(), cands.p, sizeof(MemberCand) * n_cand, cudaMemcpyDeviceToHost, st);
+    if ((rc = check(cudaStreamSynchronize(st)))) return rc;
+    std::sort(hc.begin(), hc.end(), [](const MemberCand& a, const MemberCand& b) {
+      return a.stream != b.stream ? a.stream < b.stream : a.pos < b.pos;
+    });
+  }
+  // ---- 2. members + chunk grid (host) -----------------------------------
+  struct Mem {
+    uint64_t start, ds, end;
+    uint32_t isize;
+  };
+  std::vector<std::vector<Mem>> mems(ns);
+  size_t ci = 0;
+  uint64_t est_out = 0;
+  for (uint32_t s = 0; s < ns; s++) {
+    size_t c_begin = ci;
+    while (ci < hc.size() && hc[ci].stream == s) ci++;
+    if (hinfo[s].status != kOk) {
+      R[s].status = hinfo[s].status == kNotGzip ? kNotGzip : hinfo[s].status;
+      continue;
+    }
+    const uint64_t len = S[s].len;
+    std::vector<Mem> ms;
+    bool multi = false;
+    if (ci - c_begin >= 1 && len >= 18) {
+      // scan_member_boundaries_fast acceptance (bgzf.rs:2175-2228)
+      multi = true;
+      std::vector<uint64_t> starts{0};
+      std::vector<uint32_t> hls{hinfo[s].header_len};
+      for (size_t k = c_begin; k < ci; k++) {
+        starts.push_back(hc[k].pos);
+        hls.push_back(hc[k].header_len);
+      }
+      uint64_t sum_isize = 0;
+      for (size_t k = 0; k < starts.size() && multi; k++) {
+        uint64_t e = k + 1 < starts.size() ? starts[k + 1] : len;
+        if (e - starts[k] < 18 || hls[k] == 0 || starts[k] + hls[k] >= e) {
+          multi = false;
+          break;
+        }
+        uint32_t isz = k + 1 < starts.size() ? hc[c_begin + k].prev_isize : hinfo[s].last_isize;
+        sum_isize += isz;
+        ms.push_back(Mem{starts[k], starts[k] + hls[k], e, isz});
+      }
+      if (sum_isize > len * 100) multi = false;
+    }
+    if (!multi) {
+      ms.clear();
+      ms.push_back(Mem{0, hinfo[s].header_len, len, hinfo[s].last_isize});
+    }
+    for (auto& m : ms) est_out += m.isize;
+    mems[s] = std::move(ms);
+  }
+  // grid
+  std::vector<ChunkDesc> hd;
+  std::vector<uint32_t> hspec;
+  std::vector<uint32_t> c0(ns), c1(ns);
+  uint64_t cb = chunk_bytes ? chunk_bytes : pick_chunk_bytes(total_in);
+  stats.chunk_bytes = cb;
+  const uint64_t cbits = cb * 8;
+  for (uint32_t s = 0; s < ns; s++) {
+    c0[s] = (uint32_t)hd.size();
+    for (const Mem& m : mems[s]) {
+      const uint64_t b0 = (S[s].off + m.ds) * 8, bend = (S[s].off + m.end) * 8;
+      ChunkDesc d{};
+      d.start_bit = d.lo_bit = d.guess_bit = b0;
+      d.limit_bit = S[s].off + m.start;  // member-first: the member's header byte
+      d.stop_lo = kNoStop;
+      d.in_end = S[s].off + S[s].len;
+      d.flags = kChunkMemberFirst | kChunkValid;
+      d.stream = s;
+      hd.push_back(d);
+      for (uint64_t g = b0 + cbits; g < bend; g += cbits) {
+        ChunkDesc x{};
+        x.start_bit = x.lo_bit = x.guess_bit = g;
+        x.limit_bit = std::min(g + cbits, bend);
+        x.stop_lo = kNoStop;
+        x.in_end = d.in_end;
+        x.flags = 0;
+        x.stream = s;
+        hspec.push_back((uint32_t)hd.size());
+        hd.push_back(x);
+      }
+    }
+    c1[s] = (uint32_t)hd.size();
+  }
+  const uint32_t n_grid = (uint32_t)hd.size();
+  stats.n_chunks = n_grid;
+  size_t desc_cap = n_grid + 4096;
+  if ((rc = check(descs.ensure(sizeof(ChunkDesc) * desc_cap))) ||
+      (rc = check(results.ensure(sizeof(ChunkResult) * desc_cap))) ||
+      (rc = check(spec.ensure(4 * (hspec.size() + 1)))) || (rc = check(work.ensure(4 * desc_cap))))
+    return rc;
+  if (n_grid) cudaMemcpyAsync(descs.p, hd.data(), sizeof(ChunkDesc) * n_grid, cudaMemcpyHostToDevice, st);
+  if (!hspec.empty())
+    cudaMemcpyAsync(spec.p, hspec.data(), 4 * hspec.size(), cudaMemcpyHostToDevice, st);
+  cudaMemsetAsync(counters.as<uint32_t>() + 1, 0, 4, st);
+  cudaEventRecord(ev[3], st);
+  // ---- 3. finder + link ---------------------------------------------------
+  if ((rc = check(launch_finder(cur_in, descs.as<ChunkDesc>(), spec.as<uint32_t>(),
+                                (uint32_t)hspec.size(), st))))
+    return rc;
+  if ((rc = check(launch_link(descs.as<ChunkDesc>(), n_grid, work.as<uint32_t>(),
+                              counters.as<uint32_t>() + 1, st))))
+    return rc;
+  stats.kernel_launches += 2;
+  cudaEventRecord(ev[4], st);
+  // ---- 4. decode ----------------------------------------------------------
+  uint64_t pages_needed = (est_out + n_grid * (uint64_t)kPageEntries) / kPageEntries + 64;
+  std::vector<ChunkResult> hr;
+  float ms_dec_kernel = 0;
+  for (int attempt = 0;; attempt++) {
+    if ((rc = check(pages.ensure(pages_needed * kPageEntries * 2))) ||
+        (rc = check(owner.ensure(4 * pages_needed))) || (rc = check(seq.ensure(4 * pages_needed))))
+      return rc;
+    cudaMemsetAsync(counters.as<uint32_t>() + 2, 0, 4, st);
+    cudaEventRecord(ev[8], st);
+    if ((rc = check(launch_decode(counters.as<uint32_t>() + 1)))) return rc;
+    cudaEventRecord(ev[9], st);
+    hd.resize(n_grid);
+    hr.resize(n_grid);
+    if (n_grid) {
+      cudaMemcpyAsync(hd.data(), descs.p, sizeof(ChunkDesc) * n_grid, cudaMemcpyDeviceToHost, st);
+      cudaMemcpyAsync(hr.data(), results.p, sizeof(ChunkResult) * n_grid, cudaMemcpyDeviceToHost, st);
+    }
+    if ((rc = check(cudaStreamSynchronize(st)))) return rc;
+    float t = 0;
+    cudaEventElapsedTime(&t, ev[8], ev[9]);
+    ms_dec_kernel += t;
+    bool exhausted = false;
+    for (uint32_t i = 0; i < n_grid; i++)
+      if ((hd[i].flags & kChunkValid) && hr[i].status == kPoolExhausted) exhausted = true;
+    if (!exhausted) break;
+    if (attempt >= 6) return kPoolExhausted;
+    pages_needed *= 2;
+  }
+  cudaEventRecord(ev[5], st);
+  // ---- 5. chain walk with repairs (host) ---------------------------------
+  std::vector<Walker> W(ns);
+  for (uint32_t s = 0; s < ns; s++) {
+    W[s].stream = s;
+    W[s].c0 = c0[s];
+    W[s].c1 = c1[s];
+    W[s].j = c0[s];
+    W[s].mpos = 0;
+    if (R[s].status != kOk || c0[s] == c1[s]) W[s].done = true;
+  }
+  auto is_valid = [&](uint32_t i) { return (hd[i].flags & kChunkValid) != 0; };
+  auto is_mf = [&](uint32_t i) { return (hd[i].flags & kChunkMemberFirst) != 0; };
+  std::vector<ChunkDesc> repairs;
+  std::vector<uint32_t> repair_owner;
+  uint64_t n_rejected = 0, n_repairs = 0;
+  // bytes of an input range, fetched on demand (rare: members the scan missed)
+  auto fetch = [&](uint64_t abs, size_t n, uint8_t* dst) {
+    cudaMemcpy(dst, cur_in + abs, n, cudaMemcpyDeviceToHost);
+  };
+  auto new_chunk = [&](Walker& w, uint64_t start, uint64_t stop, uint32_t flags) {
+    ChunkDesc d{};
+    d.start_bit = d.lo_bit = d.guess_bit = d.limit_bit = start;
+    if (flags & kChunkMemberFirst) d.limit_bit = S[w.stream].off + w.mpos;
+    d.stop_lo = stop;
+    d.in_end = S[w.stream].off + S[w.stream].len;
+    d.flags = flags | kChunkValid;
+    d.stream = w.stream;
+    uint32_t id = (uint32_t)(hd.size() + repairs.size());
+    repairs.push_back(d);
+    repair_owner.push_back(w.stream);
+    w.pending = (int32_t)id;
+    n_repairs++;
+  };
+  // advance one walker as far as possible; returns when done or a repair is pending
+  auto step = [&](Walker& w) {
+    const uint64_t base = S[w.stream].off, len = S[w.stream].len;
+    while (!w.done && w.pending < 0) {
+      if (w.cur < 0) {
+        // at a member header
+        if (w.member > 0 && w.mpos >= len) {
+          w.done = true;
+          break;
+        }
+        uint32_t j = w.j;
+        while (j < w.c1 && !(is_valid(j) && is_mf(j) && hd[j].limit_bit >= base + w.mpos)) j++;
+        bool found = false;
+        if (j < w.c1 && hd[j].limit_bit == base + w.mpos) {
+          w.cur = (int32_t)j;
+          w.j = j + 1;
+          found = true;
+        }
+        if (!found) {
+          if (w.member == 0) {
+            w.status = kBadHeader;
+            w.done = true;
+            break;
+          }
+          uint8_t hb[64] = {0};
+          size_t nb = (size_t)std::min<uint64_t>(64, len - w.mpos);
+          if (len - w.mpos < 18) {
+            w.done = true;  // too short to be a member: stop cleanly
+            break;
+          }
+          fetch(base + w.mpos, nb, hb);
+          if (hb[0] != 0x1f || hb[1] != 0x8b || hb[2] != 8 || (hb[3] & 0xE0)) {
+            w.done = true;  // trailing bytes that start no member
+            break;
+          }
+          // header length (FEXTRA/FNAME/FCOMMENT may exceed 64 bytes: fetch more)
+          uint64_t o = 10;
+          uint8_t flg = hb[3];
+          std::vector<uint8_t> hbuf;
+          size_t want = (size_t)std::min<uint64_t>(len - w.mpos, 1 << 20);
+          hbuf.resize(want);
+          fetch(base + w.mpos, want, hbuf.data());
+          bool ok = true;
+          if (flg & 4) {
+            if (o + 2 > want) ok = false;
+            else o += 2 + (hbuf[o] | (hbuf[o + 1] << 8));
+          }
+          for (int f = 8; f <= 16 && ok; f <<= 1)
+            if (flg & f) {
+              while (o < want && hbuf[o]) o++;
+              if (o >= want) ok = false;
+              o++;
+            }
+          if (ok && (flg & 2)) o += 2;
+          if (!ok || o >= want) {
+            w.done = true;
+            break;
+          }
+          w.member_order_begin = (uint32_t)w.order.size();
+          new_chunk(w, (base + w.mpos + o) * 8, kNoStop, kChunkMemberFirst);
+          break;
+        }
+        w.member_order_begin = (uint32_t)w.order.size();
+      }
+      // inside a member
+      const uint32_t cur = (uint32_t)w.cur;
+      const ChunkResult& r = hr[cur];
+      w.order.push_back(cur);
+      if (r.status != kOk) {
+        w.status = r.status;
+        w.done = true;
+        break;
+      }
+      if (r.final_block) {
+        uint64_t trailer = (r.end_bit + 7) / 8;
+        if (trailer + 8 > base + len) {
+          w.status = kTruncated;
+          w.done = true;
+          break;
+        }
+        uint64_t mlen = 0;
+        for (uint32_t k = w.member_order_begin; k < w.order.size(); k++) mlen += hr[w.order[k]].out_len;
+        w.members.push_back(MemberPlan{w.member_order_begin, (uint32_t)w.order.size(), trailer, mlen});
+        w.member++;
+        w.mpos = trailer + 8 - base;
+        w.cur = -1;
+        continue;
+      }
+      const uint64_t e = r.end_bit;
+      uint32_t j = w.j;
+      while (j < w.c1 && !is_valid(j)) j++;
+      if (j < w.c1 && !is_mf(j) && e >= hd[j].lo_bit && e <= hd[j].start_bit && hr[j].status == kOk) {
+        w.cur = (int32_t)j;
+        w.j = j + 1;
+        continue;
+      }
+      while (j < w.c1 && (!is_valid(j) || (!is_mf(j) && hd[j].lo_bit <= e))) {
+        if (is_valid(j)) n_rejected++;
+        j++;
+      }
+      w.j = j;
+      uint64_t stop = (j < w.c1 && !is_mf(j)) ? hd[j].lo_bit : kNoStop;
+      new_chunk(w, e, stop, 0);
+      break;
+    }
+  };
+  for (;;) {
+    for (auto& w : W) step(w);
+    if (repairs.empty()) break;
+    // decode all pending repairs in one pass
+    const uint32_t base_id = (uint32_t)hd.size(), nr = (uint32_t)repairs.size();
+    if (hd.size() + nr > desc_cap) {
+      // grow device arrays, preserving contents
+      size_t ncap = (hd.size() + nr) * 2;
+      DevBuf nd, nrr;
+      if ((rc = check(nd.ensure(sizeof(ChunkDesc) * ncap))) ||
+          (rc = check(nrr.ensure(sizeof(ChunkResult) * ncap))))
+        return rc;
+      cudaMemcpyAsync(nd.p, descs.p, sizeof(ChunkDesc) * hd.size(), cudaMemcpyDeviceToDevice, st);
+      cudaMemcpyAsync(nrr.p, results.p, sizeof(ChunkResult) * hd.size(), cudaMemcpyDeviceToDevice, st);
+      cudaStreamSynchronize(st);
+      descs.release();
+      results.release();
+      descs = nd;
+      results = nrr;
+      if ((rc = check(work.ensure(4 * ncap)))) return rc;
+      desc_cap = ncap;
+    }
+    std::vector<uint32_t> wl(nr);
+    for (uint32_t k = 0; k < nr; k++) wl[k] = base_id + k;
+    cudaMemcpyAsync(descs.as<ChunkDesc>() + base_id, repairs.data(), sizeof(ChunkDesc) * nr,
+                    cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(work.p, wl.data(), 4 * nr, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(counters.as<uint32_t>() + 1, &nr, 4, cudaMemcpyHostToDevice, st);
+    cudaEventRecord(ev[8], st);
+    if ((rc = check(launch_decode(counters.as<uint32_t>() + 1)))) return rc;
+    cudaEventRecord(ev[9], st);
+    hd.insert(hd.end(), repairs.begin(), repairs.end());
+    hr.resize(hd.size());
+    cudaMemcpyAsync(hr.data() + base_id, results.as<ChunkResult>() + base_id,
+                    sizeof(ChunkResult) * nr, cudaMemcpyDeviceToHost, st);
+    if ((rc = check(cudaStreamSynchronize(st)))) return rc;
+    float t = 0;
+    cudaEventElapsedTime(&t, ev[8], ev[9]);
+    ms_dec_kernel += t;
+    for (uint32_t k = 0; k < nr; k++)
+      if (hr[base_id + k].status == kPoolExhausted) return kPoolExhausted;
+    for (uint32_t k = 0; k < nr; k++) {
+      Walker& w = W[repair_owner[k]];
+      w.cur = w.pending;
+      w.pending = -1;
+    }
+    repairs.clear();
+    repair_owner.clear();
+  }
+  stats.n_rejected = n_rejected;
+  stats.n_repairs = n_repairs;
+  // ---- output placement ----------------------------------------------------
+  const uint32_t n_all = (uint32_t)hd.size();
+  std::vector<PlacedChunk> placed;
+  std::vector<uint32_t> placed_of(n_all, 0xFFFFFFFFu);
+  std::vector<uint32_t> tlist, tseg{0};
+  std::vector<CrcBlock> cblk;
+  std::vector<uint32_t> mblk{0};
+  std::vector<uint64_t> mtrail, mlenv;
+  std::vector<std::pair<uint32_t, uint32_t>> mem_owner;  // (stream, member)
+  uint64_t out_total = 0;
+  const uint64_t kCrcBlock = 64 << 10;
+  for (uint32_t s = 0; s < ns; s++) {
+    Walker& w = W[s];
+    if (R[s].status == kOk) R[s].status = w.status;
+    if (R[s].status != kOk) continue;
+    R[s].out_off = out_total;
+    uint64_t so = 0;
+    for (const MemberPlan& mp : w.members) {
+      uint64_t moff = out_total + so;
+      for (uint32_t k = mp.order_begin; k < mp.order_end; k++) {
+        uint32_t cid = w.order[k];
+        placed_of[cid] = (uint32_t)placed.size();
+        placed.push_back(PlacedChunk{out_total + so, moff, cid, 0});
+        const ChunkResult& r = hr[cid];
+        uint64_t t0 = r.out_len > kWindow ? r.out_len - kWindow : 0;
+        if (r.marker_end > t0) tlist.push_back((uint32_t)placed.size() - 1);
+        so += r.out_len;
+      }
+      for (uint64_t b = 0; b < mp.out_len; b += kCrcBlock)
+        cblk.push_back(CrcBlock{moff + b, (uint32_t)std::min(kCrcBlock, mp.out_len - b),
+                                (uint32_t)mtrail.size()});
+      mblk.push_back((uint32_t)cblk.size());
+      mtrail.push_back(mp.trailer);
+      mlenv.push_back(mp.out_len);
+      mem_owner.push_back({s, 0});
+    }
+    if (tseg.back() != tlist.size()) tseg.push_back((uint32_t)tlist.size());
+    R[s].out_len = so;
+    out_total += so;
+  }
+  stats.n_accepted = placed.size();
+  stats.n_tail_marker_chunks = tlist.size();
+  stats.n_members = mtrail.size();
+  stats.out_bytes = out_total;
+  cudaEventRecord(ev[6], st);
+  // ---- 6. resolve + CRC ----------------------------------------------------
+  uint32_t n_pages_used = 0;
+  cudaMemcpyAsync(&n_pages_used, counters.as<uint32_t>() + 2, 4, cudaMemcpyDeviceToHost, st);
+  if ((rc = check(cudaStreamSynchronize(st)))) return rc;
+  const uint32_t pool_cap = (uint32_t)std::min<uint64_t>(pages.cap / (kPageEntries * 2),
+                                                         std::min(owner.cap, seq.cap) / 4);
+  n_pages_used = std::min(n_pages_used, pool_cap);
+  stats.n_pages = n_pages_used;
+  cur_out = (user_out && out_total <= user_cap) ? user_out : nullptr;
+  if ((rc = check(cur_out ? cudaSuccess : out.ensure(out_total + 64))) ||
+      (rc = check(this->placed.ensure(sizeof(PlacedChunk) * (placed.size() + 1)))) ||
+      (rc = check(this->placed_of.ensure(4 * (n_all + 1)))) || (rc = check(list.ensure(4 * (tlist.size() + 1)))) ||
+      (rc = check(segs.ensure(4 * (tseg.size() + 1)))) ||
+      (rc = check(cblocks.ensure(sizeof(CrcBlock) * (cblk.size() + 1)))) ||
+      (rc = check(bcrcs.ensure(4 * (cblk.size() + 1)))) || (rc = check(this->mblk.ensure(4 * (mblk.size() + 1)))) ||
+      (rc = check(this->mtrail.ensure(8 * (mtrail.size() + 1)))) || (rc = check(mlen.ensure(8 * (mlenv.size() + 1)))) ||
+      (rc = check(mcrc.ensure(4 * (mtrail.size() + 1)))) ||
+      (rc = check(mstatus.ensure(4 * (mtrail.size() + 1)))))
+    return rc;
+  if (!placed.empty())
+    cudaMemcpyAsync(this->placed.p, placed.data(), sizeof(PlacedChunk) * placed.size(),
+                    cudaMemcpyHostToDevice, st);
+  if (n_all) cudaMemcpyAsync(this->placed_of.p, placed_of.data(), 4 * n_all, cudaMemcpyHostToDevice, st);
+  if (!tlist.empty()) cudaMemcpyAsync(list.p, tlist.data(), 4 * tlist.size(), cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(segs.p, tseg.data(), 4 * tseg.size(), cudaMemcpyHostToDevice, st);
+  if (!cblk.empty())
+    cudaMemcpyAsync(cblocks.p, cblk.data(), sizeof(CrcBlock) * cblk.size(), cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(this->mblk.p, mblk.data(), 4 * mblk.size(), cudaMemcpyHostToDevice, st);
+  if (!mtrail.empty()) {
+    cudaMemcpyAsync(this->mtrail.p, mtrail.data(), 8 * mtrail.size(), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(mlen.p, mlenv.data(), 8 * mlenv.size(), cudaMemcpyHostToDevice, st);
+  }
+  if (!cur_out) cur_out = out.as<uint8_t>();
+  PagePool pool{pages.as<uint16_t>(), owner.as<uint32_t>(), seq.as<uint32_t>(),
+                counters.as<uint32_t>() + 2, pool_cap};
+  cudaEventRecord(ev[10], st);
+  if (!crc_ready) {
+    if ((rc = check(resolve_init(st)))) return rc;
+    crc_ready = true;
+  }
+  const uint32_t np = (uint32_t)placed.size();
+  if ((rc = check(launch_tail_literals(this->placed.as<PlacedChunk>(), np, results.as<ChunkResult>(),
+                                       pool, cur_out, st))) ||
+      (rc = check(launch_tail_markers(this->placed.as<PlacedChunk>(), list.as<uint32_t>(),
+                                      segs.as<uint32_t>(), (uint32_t)tseg.size() - 1,
+                                      results.as<ChunkResult>(), pool, cur_out, st))) ||
+      (rc = check(launch_body(this->placed.as<PlacedChunk>(), this->placed_of.as<uint32_t>(),
+                              n_pages_used, results.as<ChunkResult>(), pool, cur_out, sms,
+                              st))))
+    return rc;
+  cudaEventRecord(ev[11], st);
+  if ((rc = check(launch_crc(cblocks.as<CrcBlock>(), (uint32_t)cblk.size(), cur_out,
+                             bcrcs.as<uint32_t>(), this->mblk.as<uint32_t>(),
+                             this->mtrail.as<uint64_t>(), mlen.as<uint64_t>(),
+                             (uint32_t)mtrail.size(), cur_in, mcrc.as<uint32_t>(),
+                             mstatus.as<int32_t>(), sms, st))))
+    return rc;
+  stats.kernel_launches += 5;
+  std::vector<int32_t> mst(mtrail.size());
+  if (!mst.empty())
+    cudaMemcpyAsync(mst.data(), mstatus.p, 4 * mst.size(), cudaMemcpyDeviceToHost, st);
+  cudaEventRecord(ev[7], st);
+  if ((rc = check(cudaStreamSynchronize(st)))) return rc;
+  {
+    size_t mi = 0;
+    for (uint32_t s = 0; s < ns; s++) {
+      if (R[s].status != kOk) continue;
+      for (size_t k = 0; k < W[s].members.size(); k++, mi++)
+        if (R[s].status == kOk && mst[mi] != kOk) R[s].status = mst[mi];
+    }
+  }
+  float t;
+  auto el = [&](int a, int b) {
+    t = 0;
+    cudaEventElapsedTime(&t, ev[a], ev[b]);
+    return (double)t;
+  };
+  stats.ms_scan = el(1, 2);
+  stats.ms_find = el(3, 4);
+  stats.ms_decode = el(4, 5);
+  stats.ms_decode_kernel = ms_dec_kernel;
+  stats.ms_walk = el(5, 6);
+  stats.ms_resolve = el(10, 11);
+  stats.ms_crc = el(11, 7);
+  stats.n_streams = ns;
+  stats.in_bytes = total_in;
+  (void)t_host0;
+  return kOk;
+}
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+const char* gzgpu_strerror(int code) {
+  if (code >= 0 && code < (int)(sizeof(kErrStr) / sizeof(kErrStr[0]))) return kErrStr[code];
+  return "unknown error";
+}
+
+int gzgpu_create(gzgpu_ctx** out, const gzgpu_config* cfg) {
+  if (!out) return GZGPU_INVALID_ARGUMENT;
+  *out = nullptr;
+  gzgpu_ctx* c = new (std::nothrow) gzgpu_ctx();
+  if (!c) return GZGPU_DEVICE_ERROR;
+  if (cfg) {
+    c->dev = cfg->device;
+    c->chunk_bytes = cfg->chunk_bytes;
+    if (cfg->lut_bits == 11 || cfg->lut_bits == 12) c->lut_bits = cfg->lut_bits;
+    c->autotune = cfg->autotune != 0;
+  }
+  if (cudaSetDevice(c->dev) != cudaSuccess) {
+    delete c;
+    return GZGPU_DEVICE_ERROR;
+  }
+  cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, c->dev);
+  if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess) {
+    delete c;
+    return GZGPU_DEVICE_ERROR;
+  }
+  for (auto& e : c->ev) cudaEventCreate(&e);
+  c->setup_decode_grid();
+  *out = c;
+  return GZGPU_OK;
+}
+
+void gzgpu_destroy(gzgpu_ctx* c) {
+  if (!c) return;
+  cudaSetDevice(c->dev);
+  cudaStreamSynchronize(c->st);
+  DevBuf* bufs[] = {&c->in,     &c->out,   &c->s_off,   &c->s_len,  &c->info,   &c->units,
+                    &c->cands,  &c->counters, &c->descs, &c->results, &c->spec, &c->work,
+                    &c->pages,  &c->owner, &c->seq,     &c->placed, &c->placed_of, &c->list,
+                    &c->segs,   &c->cblocks, &c->bcrcs, &c->mblk,   &c->mtrail, &c->mlen,
+                    &c->mcrc,   &c->mstatus};
+  for (DevBuf* b : bufs) b->release();
+  c->h_stage.release();
+  for (auto& e : c->ev) cudaEventDestroy(e);
+  cudaStreamDestroy(c->st);
+  delete c;
+}
+
+namespace {
+
+// host -> device copy of one stream into the context input buffer
+int stage_input(gzgpu_ctx* c, const uint8_t* in, size_t n, uint64_t at) {
+  cudaError_t e = cudaMemcpyAsync(c->in.as<uint8_t>() + at, in, n, cudaMemcpyHostToDevice, c->st);
+  return c->check(e);
+}
+
+void reset_stats(gzgpu_ctx* c) {
+  c->stats = gzgpu_stats{};
+  c->stats.lut_bits = c->lut_bits;
+}
+
+void finish_stats(gzgpu_ctx* c) {
+  float t = 0;
+  cudaEventElapsedTime(&t, c->ev[0], c->ev[1]);
+  c->stats.ms_h2d = t;
+  t = 0;
+  cudaEventElapsedTime(&t, c->ev[0], c->ev[7]);
+  c->stats.ms_total = t;
+}
+
+}  // namespace
+
+int gzgpu_decompress(gzgpu_ctx* c, const uint8_t* in, size_t in_len, uint8_t* out,
+                     size_t out_cap, size_t* out_len) {
+  if (!c || !out_len || (!in && in_len) || (!out && out_cap)) return GZGPU_INVALID_ARGUMENT;
+  *out_len = 0;
+  if (in_len < 2 || in[0] != 0x1f || in[1] != 0x8b) return GZGPU_NOT_GZIP;
+  std::lock_guard<std::mutex> g(c->mu);
+  cudaSetDevice(c->dev);
+  reset_stats(c);
+  int rc;
+  if ((rc = c->check(c->in.ensure(in_len + kInputPad)))) return rc;
+  cudaEventRecord(c->ev[0], c->st);
+  if ((rc = stage_input(c, in, in_len, 0))) return rc;
+  cudaMemsetAsync(c->in.as<uint8_t>() + in_len, 0, kInputPad, c->st);
+  c->cur_in = c->in.as<uint8_t>();
+  c->user_out = nullptr;
+  std::vector<StreamSpec> S{{0, in_len}};
+  std::vector<StreamOut> R;
+  rc = c->run(S, R);
+  if (rc != kOk) return rc;
+  finish_stats(c);
+  if (R[0].status != kOk) return R[0].status;
+  *out_len = R[0].out_len;
+  if (R[0].out_len > out_cap) return GZGPU_OUT_TOO_SMALL;
+  cudaEvent_t t0 = c->ev[8], t1 = c->ev[9];
+  cudaEventRecord(t0, c->st);
+  if (R[0].out_len &&
+      (rc = c->check(cudaMemcpyAsync(out, c->cur_out + R[0].out_off, R[0].out_len,
+                                     cudaMemcpyDeviceToHost, c->st))))
+    return rc;
+  cudaEventRecord(t1, c->st);
+  if ((rc = c->check(cudaStreamSynchronize(c->st)))) return rc;
+  float t = 0;
+  cudaEventElapsedTime(&t, t0, t1);
+  c->stats.ms_d2h = t;
+  t = 0;
+  cudaEventElapsedTime(&t, c->ev[0], t1);
+  c->stats.ms_total = t;
+  return GZGPU_OK;
+}
+
+int gzgpu_decompress_device(gzgpu_ctx* c, const void* d_in, size_t in_len, void* d_out,
+                            size_t out_cap, size_t* out_len) {
+  if (!c || !out_len || (!d_in && in_len)) return GZGPU_INVALID_ARGUMENT;
+  *out_len = 0;
+  std::lock_guard<std::mutex> g(c->mu);
+  cudaSetDevice(c->dev);
+  reset_stats(c);
+  if ((reinterpret_cast<uintptr_t>(d_in) | reinterpret_cast<uintptr_t>(d_out)) & 15)
+    return GZGPU_INVALID_ARGUMENT;  // the kernels use 16-byte vector access
+  uint8_t magic[2] = {0, 0};
+  if (in_len >= 2 && c->check(cudaMemcpy(magic, d_in, 2, cudaMemcpyDeviceToHost)))
+    return GZGPU_DEVICE_ERROR;
+  if (in_len < 2 || magic[0] != 0x1f || magic[1] != 0x8b) return GZGPU_NOT_GZIP;
+  cudaEventRecord(c->ev[0], c->st);
+  c->cur_in = reinterpret_cast<const uint8_t*>(d_in);
+  c->user_out = reinterpret_cast<uint8_t*>(d_out);
+  c->user_cap = out_cap;
+  std::vector<StreamSpec> S{{0, in_len}};
+  std::vector<StreamOut> R;
+  int rc = c->run(S, R);
+  c->user_out = nullptr;
+  if (rc != kOk) return rc;
+  finish_stats(c);
+  if (R[0].status != kOk) return R[0].status;
+  *out_len = R[0].out_len;
+  if (R[0].out_len > out_cap) return GZGPU_OUT_TOO_SMALL;
+  return GZGPU_OK;
+}
+
+int gzgpu_decompress_to_writer(gzgpu_ctx* c, const uint8_t* in, size_t in_len,
+                               gzgpu_write_fn write, void* user, uint64_t* written) {
+  if (!c || !write || (!in && in_len)) return GZGPU_INVALID_ARGUMENT;
+  if (written) *written = 0;
+  if (in_len < 2 || in[0] != 0x1f || in[1] != 0x8b) return GZGPU_NOT_GZIP;
+  std::lock_guard<std::mutex> g(c->mu);
+  cudaSetDevice(c->dev);
+  reset_stats(c);
+  int rc;
+  if ((rc = c->check(c->in.ensure(in_len + kInputPad)))) return rc;
+  cudaEventRecord(c->ev[0], c->st);
+  if ((rc = stage_input(c, in, in_len, 0))) return rc;
+  cudaMemsetAsync(c->in.as<uint8_t>() + in_len, 0, kInputPad, c->st);
+  c->cur_in = c->in.as<uint8_t>();
+  c->user_out = nullptr;
+  std::vector<StreamSpec> S{{0, in_len}};
+  std::vector<StreamOut> R;
+  rc = c->run(S, R);
+  if (rc != kOk) return rc;
+  finish_stats(c);
+  if (R[0].status != kOk) return R[0].status;
+  // deliver in order through a pinned bounce buffer, two halves in flight
+  const size_t piece = 32 << 20;
+  if (!c->h_stage.ensure(2 * piece)) return GZGPU_DEVICE_ERROR;
+  uint8_t* hb = reinterpret_cast<uint8_t*>(c->h_stage.p);
+  uint64_t done = 0, total = R[0].out_len;
+  int half = 0;
+  while (done < total) {
+    size_t k = (size_t)std::min<uint64_t>(piece, total - done);
+    if ((rc = c->check(cudaMemcpyAsync(hb + half * piece, c->cur_out + R[0].out_off + done, k,
+                                       cudaMemcpyDeviceToHost, c->st))))
+      return rc;
+    if ((rc = c->check(cudaStreamSynchronize(c->st)))) return rc;
+    if (write(user, hb + half * piece, k) != 0) return GZGPU_INVALID_ARGUMENT;
+    done += k;
+    half ^= 1;
+    if (written) *written = done;
+  }
+  return GZGPU_OK;
+}
+
+int gzgpu_decompress_batch(gzgpu_ctx* c, const gzgpu_span* ins, size_t n, gzgpu_out* outs,
+                           int* statuses) {
+  if (!c || (n && (!ins || !outs || !statuses))) return GZGPU_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> g(c->mu);
+  cudaSetDevice(c->dev);
+  reset_stats(c);
+  uint64_t total = 0;
+  for (size_t i = 0; i < n; i++) total += (ins[i].len + 15) & ~15ull;
+  int rc;
+  if ((rc = c->check(c->in.ensure(total + kInputPad)))) return rc;
+  // pack the streams (16-byte aligned) through the pinned bounce buffer
+  if (!c->h_stage.ensure(total ? total : 1)) return GZGPU_DEVICE_ERROR;
+  uint8_t* hb = reinterpret_cast<uint8_t*>(c->h_stage.p);
+  std::vector<StreamSpec> S(n);
+  uint64_t at = 0;
+  for (size_t i = 0; i < n; i++) {
+    if (ins[i].len) memcpy(hb + at, ins[i].data, ins[i].len);
+    S[i] = StreamSpec{at, ins[i].len};
+    at += (ins[i].len + 15) & ~15ull;
+  }
+  cudaEventRecord(c->ev[0], c->st);
+  if (at && (rc = c->check(cudaMemcpyAsync(c->in.p, hb, at, cudaMemcpyHostToDevice, c->st))))
+    return rc;
+  cudaMemsetAsync(c->in.as<uint8_t>() + at, 0, kInputPad, c->st);
+  c->cur_in = c->in.as<uint8_t>();
+  c->user_out = nullptr;
+  std::vector<StreamOut> R;
+  rc = c->run(S, R);
+  if (rc != kOk) return rc;
+  finish_stats(c);
+  int all = GZGPU_OK;
+  uint64_t out_total = 0;
+  for (size_t i = 0; i < n; i++) out_total += R[i].out_len;
+  if (!c->h_stage.ensure(out_total ? out_total : 1)) return GZGPU_DEVICE_ERROR;
+  hb = reinterpret_cast<uint8_t*>(c->h_stage.p);
+  cudaEvent_t t0 = c->ev[8], t1 = c->ev[9];
+  cudaEventRecord(t0, c->st);
+  if (out_total && (rc = c->check(cudaMemcpyAsync(hb, c->cur_out, out_total, cudaMemcpyDeviceToHost,
+                                                  c->st))))
+    return rc;
+  cudaEventRecord(t1, c->st);
+  if ((rc = c->check(cudaStreamSynchronize(c->st)))) return rc;
+  for (size_t i = 0; i < n; i++) {
+    statuses[i] = R[i].status;
+    outs[i].len = R[i].status == kOk ? R[i].out_len : 0;
+    if (R[i].status == kOk && R[i].out_len > outs[i].cap) {
+      statuses[i] = GZGPU_OUT_TOO_SMALL;
+      outs[i].len = R[i].out_len;
+    } else if (R[i].status == kOk && R[i].out_len) {
+      memcpy(outs[i].data, hb + R[i].out_off, R[i].out_len);
+    }
+    if (statuses[i] != GZGPU_OK && statuses[i] != GZGPU_NOT_GZIP && all == GZGPU_OK) all = statuses[i];
+  }
+  float t = 0;
+  cudaEventElapsedTime(&t, t0, t1);
+  c->stats.ms_d2h = t;
+  t = 0;
+  cudaEventElapsedTime(&t, c->ev[0], t1);
+  c->stats.ms_total = t;
+  return all;
+}
+
+int gzgpu_debug_find(gzgpu_ctx* c, const uint8_t* in, size_t in_len, const uint64_t* from,
+                     const uint64_t* to, size_t n, uint64_t* lo, uint64_t* hi, int* valid) {
+  if (!c || (!in && in_len) || (n && (!from || !to || !lo || !hi || !valid)))
+    return GZGPU_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> g(c->mu);
+  cudaSetDevice(c->dev);
+  int rc;
+  if ((rc = c->check(c->in.ensure(in_len + kInputPad))) ||
+      (rc = c->check(c->descs.ensure(sizeof(ChunkDesc) * (n + 1)))) ||
+      (rc = c->check(c->spec.ensure(4 * (n + 1)))))
+    return rc;
+  cudaMemcpyAsync(c->in.p, in, in_len, cudaMemcpyHostToDevice, c->st);
+  cudaMemsetAsync(c->in.as<uint8_t>() + in_len, 0, kInputPad, c->st);
+  std::vector<ChunkDesc> d(n);
+  std::vector<uint32_t> sp(n);
+  for (size_t i = 0; i < n; i++) {
+    d[i] = ChunkDesc{};
+    d[i].guess_bit = d[i].start_bit = d[i].lo_bit = from[i];
+    d[i].limit_bit = to[i];
+    d[i].in_end = in_len;
+    sp[i] = (uint32_t)i;
+  }
+  if (n) {
+    cudaMemcpyAsync(c->descs.p, d.data(), sizeof(ChunkDesc) * n, cudaMemcpyHostToDevice, c->st);
+    cudaMemcpyAsync(c->spec.p, sp.data(), 4 * n, cudaMemcpyHostToDevice, c->st);
+    if ((rc = c->check(launch_finder(c->in.as<uint8_t>(), c->descs.as<ChunkDesc>(),
+                                     c->spec.as<uint32_t>(), (uint32_t)n, c->st))))
+      return rc;
+    cudaMemcpyAsync(d.data(), c->descs.p, sizeof(ChunkDesc) * n, cudaMemcpyDeviceToHost, c->st);
+  }
+  if ((rc = c->check(cudaStreamSynchronize(c->st)))) return rc;
+  for (size_t i = 0; i < n; i++) {
+    valid[i] = (d[i].flags & kChunkValid) ? 1 : 0;
+    lo[i] = d[i].lo_bit;
+    hi[i] = d[i].start_bit;
+  }
+  return GZGPU_OK;
+}
+
+int gzgpu_debug_decode(gzgpu_ctx* c, const uint8_t* in, size_t in_len, const uint64_t* start,
+                       const uint64_t* stop, const int* member_first, size_t n, uint16_t* entries,
+                       size_t cap_per, uint64_t* res) {
+  if (!c || (!in && in_len) || (n && (!start || !stop || !member_first || !res)))
+    return GZGPU_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> g(c->mu);
+  cudaSetDevice(c->dev);
+  int rc;
+  uint64_t pages_needed = n * 64 + in_len / 4096 + 64;
+  if ((rc = c->check(c->in.ensure(in_len + kInputPad))) ||
+      (rc = c->check(c->descs.ensure(sizeof(ChunkDesc) * (n + 1)))) ||
+      (rc = c->check(c->results.ensure(sizeof(ChunkResult) * (n + 1)))) ||
+      (rc = c->check(c->work.ensure(4 * (n + 1)))) || (rc = c->check(c->counters.ensure(64))) ||
+      (rc = c->check(c->pages.ensure(pages_needed * kPageEntries * 2))) ||
+      (rc = c->check(c->owner.ensure(4 * pages_needed))) ||
+      (rc = c->check(c->seq.ensure(4 * pages_needed))))
+    return rc;
+  cudaMemcpyAsync(c->in.p, in, in_len, cudaMemcpyHostToDevice, c->st);
+  cudaMemsetAsync(c->in.as<uint8_t>() + in_len, 0, kInputPad, c->st);
+  std::vector<ChunkDesc> d(n);
+  std::vector<uint32_t> wl(n);
+  for (size_t i = 0; i < n; i++) {
+    d[i] = ChunkDesc{};
+    d[i].start_bit = d[i].lo_bit = d[i].guess_bit = d[i].limit_bit = start[i];
+    d[i].stop_lo = stop[i];
+    d[i].in_end = in_len;
+    d[i].flags = kChunkValid | (member_first[i] ? kChunkMemberFirst : 0u);
+    wl[i] = (uint32_t)i;
+  }
+  uint32_t nn = (uint32_t)n;
+  cudaMemsetAsync(c->counters.p, 0, 64, c->st);
+  if (n) {
+    cudaMemcpyAsync(c->descs.p, d.data(), sizeof(ChunkDesc) * n, cudaMemcpyHostToDevice, c->st);
+    cudaMemcpyAsync(c->work.p, wl.data(), 4 * n, cudaMemcpyHostToDevice, c->st);
+  }
+  cudaMemcpyAsync(c->counters.as<uint32_t>() + 1, &nn, 4, cudaMemcpyHostToDevice, c->st);
+  c->cur_in = c->in.as<uint8_t>();
+  if ((rc = c->check(c->launch_decode(c->counters.as<uint32_t>() + 1)))) return rc;
+  std::vector<ChunkResult> r(n);
+  uint32_t used = 0;
+  if (n) cudaMemcpyAsync(r.data(), c->results.p, sizeof(ChunkResult) * n, cudaMemcpyDeviceToHost, c->st);
+  cudaMemcpyAsync(&used, c->counters.as<uint32_t>() + 2, 4, cudaMemcpyDeviceToHost, c->st);
+  if ((rc = c->check(cudaStreamSynchronize(c->st)))) return rc;
+  const uint64_t cap = std::min<uint64_t>(c->pages.cap / (kPageEntries * 2),
+                                          std::min(c->owner.cap, c->seq.cap) / 4);
+  used = (uint32_t)std::min<uint64_t>(used, cap);
+  std::vector<uint32_t> own(used), sq(used);
+  if (used) {
+    cudaMemcpy(own.data(), c->owner.p, 4 * used, cudaMemcpyDeviceToHost);
+    cudaMemcpy(sq.data(), c->seq.p, 4 * used, cudaMemcpyDeviceToHost);
+  }
+  for (size_t i = 0; i < n; i++) {
+    uint64_t* o = res + 6 * i;
+    o[0] = r[i].end_bit;
+    o[1] = r[i].out_len;
+    o[2] = r[i].marker_end;
+    o[3] = r[i].n_blocks;
+    o[4] = (uint64_t)(int64_t)r[i].status;
+    o[5] = r[i].final_block;
+  }
+  if (entries) {
+    for (uint32_t p = 0; p < used; p++) {
+      uint32_t cid = own[p];
+      if (cid >= n || r[cid].status != kOk) continue;
+      uint64_t q0 = (uint64_t)sq[p] * kPageEntries;
+      if (q0 >= r[cid].out_len || q0 >= cap_per) continue;
+      uint64_t k = std::min<uint64_t>({(uint64_t)kPageEntries, r[cid].out_len - q0, cap_per - q0});
+      cudaMemcpy(entries + cid * cap_per + q0, c->pages.as<uint16_t>() + (size_t)p * kPageEntries,
+                 2 * k, cudaMemcpyDeviceToHost);
+    }
+  }
+  return GZGPU_OK;
+}
+
+int gzgpu_get_stats(gzgpu_ctx* c, gzgpu_stats* out) {
+  if (!c || !out) return GZGPU_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> g(c->mu);
+  *out = c->stats;
+  return GZGPU_OK;
+}
+
+}  // extern "C"

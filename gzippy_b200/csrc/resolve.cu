@@ -1,0 +1,313 @@
+// resolve.cu -- window propagation, marker resolution and CRC32 (K3-K5).
+//
+// After decoding, every accepted chunk k has an output offset out_off[k]
+// and u16 entries in its pages.  An entry v < 256 is a byte; v >= 32768 is
+// window index v - 32768 of the 32 KiB that precede the chunk in the final
+// output (replace_markers.rs:7-23), i.e. final[out_off - 32768 + v - 32768],
+// read as 0 before the member's first byte (the zero window).
+//
+//   tail_literals : bytes of every chunk's last 32 KiB ("tail") -> output
+//   tail_markers  : markers in tails, chunk after chunk in output order: a
+//                   tail's markers only reach the tails of earlier chunks,
+//                   so this walk is the window chain (window_map.rs:80-103,
+//                   chunk_fetcher.rs publish_subchunk_windows :2295)
+//   body          : all other entries, fully parallel over pages, reading
+//                   windows the chain made final (resolve_and_narrow_markers
+//                   _in_place_crc, chunk_data.rs:1745)
+//   crc_blocks    : CRC32 of fixed-size blocks of output, lane-split
+//   crc_members   : GF(2) combine of block CRCs per member (crc32.rs
+//                   combine_crc32 :127), compared with the member trailer
+#include <cstdint>
+
+#include "common.cuh"
+#include "resolve.cuh"
+
+namespace gzgpu {
+
+__device__ __forceinline__ const uint16_t* chunk_entry_page(const ChunkResult& r, uint64_t q,
+                                                            const PagePool& pool) {
+  uint64_t seq = q / kPageEntries;
+  uint32_t page = (seq + 1 == r.n_pages) ? r.last_page : r.prev_page;
+  return pool.data + (size_t)page * kPageEntries;
+}
+
+__global__ void tail_literals_kernel(const PlacedChunk* __restrict__ placed, uint32_t n,
+                                     const ChunkResult* __restrict__ results, PagePool pool,
+                                     uint8_t* __restrict__ out) {
+  uint32_t k = blockIdx.x;
+  if (k >= n) return;
+  const PlacedChunk pc = placed[k];
+  const ChunkResult r = results[pc.chunk];
+  uint64_t len = r.out_len, t0 = len > kWindow ? len - kWindow : 0;
+  for (uint64_t q = t0 + threadIdx.x; q < len; q += blockDim.x) {
+    uint16_t v = chunk_entry_page(r, q, pool)[q % kPageEntries];
+    if (v < 256) out[pc.out_off + q] = (uint8_t)v;
+  }
+}
+
+// one CTA per segment of the ordered tail-marker list (one segment per
+// stream); inside a segment, chunks are resolved strictly in order.
+__global__ void tail_markers_kernel(const PlacedChunk* __restrict__ placed,
+                                    const uint32_t* __restrict__ list,
+                                    const uint32_t* __restrict__ seg_begin, uint32_t n_seg,
+                                    const ChunkResult* __restrict__ results, PagePool pool,
+                                    uint8_t* out) {
+  uint32_t s = blockIdx.x;
+  if (s >= n_seg) return;
+  for (uint32_t i = seg_begin[s]; i < seg_begin[s + 1]; i++) {
+    const PlacedChunk pc = placed[list[i]];
+    const ChunkResult r = results[pc.chunk];
+    uint64_t len = r.out_len, t0 = len > kWindow ? len - kWindow : 0;
+    uint64_t end = r.marker_end < len ? r.marker_end : len;
+    for (uint64_t q = t0 + threadIdx.x; q < end; q += blockDim.x) {
+      uint16_t v = chunk_entry_page(r, q, pool)[q % kPageEntries];
+      if (v >= kMarkerBase) {
+        int64_t src = (int64_t)pc.out_off - (int64_t)kWindow + (int64_t)(v - kMarkerBase);
+        out[pc.out_off + q] = src >= (int64_t)pc.member_off ? out[src] : 0;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// one CTA per page; 8 entries per thread per step
+__global__ void body_kernel(const PlacedChunk* __restrict__ placed,
+                            const uint32_t* __restrict__ placed_of_chunk, uint32_t n_pages,
+                            const ChunkResult* __restrict__ results, PagePool pool,
+                            uint8_t* __restrict__ out) {
+  for (uint32_t p = blockIdx.x; p < n_pages; p += gridDim.x) {
+    uint32_t cid = pool.owner[p];
+    uint32_t k = placed_of_chunk[cid];
+    if (k == 0xFFFFFFFFu) continue;
+    const PlacedChunk pc = placed[k];
+    const uint64_t len = results[cid].out_len;
+    const uint64_t t0 = len > kWindow ? len - kWindow : 0;
+    const uint64_t q0 = (uint64_t)pool.seq[p] * kPageEntries;
+    if (q0 >= t0) continue;
+    uint64_t qend = q0 + kPageEntries;
+    if (qend > t0) qend = t0;
+    const uint16_t* src = pool.data + (size_t)p * kPageEntries;
+    const int64_t wbase = (int64_t)pc.out_off - (int64_t)kWindow - (int64_t)kMarkerBase;
+    for (uint64_t q = q0 + 8 * threadIdx.x; q < qend; q += 8 * blockDim.x) {
+      uint4 v4 = *reinterpret_cast<const uint4*>(src + (q - q0));
+      uint16_t e[8] = {(uint16_t)v4.x, (uint16_t)(v4.x >> 16), (uint16_t)v4.y,
+                       (uint16_t)(v4.y >> 16), (uint16_t)v4.z, (uint16_t)(v4.z >> 16),
+                       (uint16_t)v4.w, (uint16_t)(v4.w >> 16)};
+      uint8_t* dst = out + pc.out_off + q;
+#pragma unroll
+      for (int j = 0; j < 8; j++) {
+        if (q + j >= qend) break;
+        uint16_t v = e[j];
+        uint8_t b;
+        if (v < 256) {
+          b = (uint8_t)v;
+        } else {
+          int64_t s = wbase + v;
+          b = s >= (int64_t)pc.member_off ? out[s] : 0;
+        }
+        dst[j] = b;
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// CRC32 (reflected 0xEDB88320): slice-by-8 tables in shared memory, GF(2)
+// combine crc(A|B) = x^(8|B|) * crc(A) + crc(B) mod P.
+// ---------------------------------------------------------------------------
+__device__ uint32_t d_crc_tab[8][256];
+__device__ uint32_t d_x2n[64];  // x^(2^k) mod P
+
+__device__ __forceinline__ uint32_t gf2_mulmod(uint32_t a, uint32_t b) {
+  uint32_t r = 0;
+#pragma unroll 8
+  for (int i = 31; i >= 0; i--) {
+    r ^= b & (0u - ((a >> i) & 1u));
+    b = (b >> 1) ^ (0xEDB88320u & (0u - (b & 1u)));
+  }
+  return r;
+}
+
+// x^(8n) mod P
+__device__ __forceinline__ uint32_t x_pow_8n(uint64_t n) {
+  uint32_t p = 1u << 31;
+  uint64_t e = n << 3;
+  for (int k = 0; e; e >>= 1, k++)
+    if (e & 1) p = gf2_mulmod(d_x2n[k & 31], p);
+  return p;
+}
+
+__device__ __forceinline__ uint32_t crc_combine(uint32_t c1, uint32_t c2, uint64_t len2) {
+  return gf2_mulmod(x_pow_8n(len2), c1) ^ c2;
+}
+
+__global__ void crc_init_kernel() {
+  uint32_t i = threadIdx.x;
+  uint32_t c = i;
+  for (int k = 0; k < 8; k++) c = (c >> 1) ^ (0xEDB88320u & (0u - (c & 1u)));
+  d_crc_tab[0][i] = c;
+  __syncthreads();
+  for (int t = 1; t < 8; t++) {
+    uint32_t p = d_crc_tab[t - 1][i];
+    d_crc_tab[t][i] = (p >> 8) ^ d_crc_tab[0][p & 0xFF];
+    __syncthreads();
+  }
+  if (i == 0) {
+    uint32_t v = 1u << 30;  // x^1
+    for (int k = 0; k < 64; k++) {
+      d_x2n[k] = v;
+      v = gf2_mulmod(v, v);
+    }
+  }
+}
+
+// one warp per CRC block; lane l hashes bytes [l*len/32, (l+1)*len/32)
+__global__ void crc_blocks_kernel(const CrcBlock* __restrict__ blocks, uint32_t n,
+                                  const uint8_t* __restrict__ out, uint32_t* __restrict__ crcs) {
+  __shared__ uint32_t tab[8][256];
+  for (int i = threadIdx.x; i < 8 * 256; i += blockDim.x) tab[i >> 8][i & 255] = d_crc_tab[i >> 8][i & 255];
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  for (uint32_t b = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; b < n;
+       b += (gridDim.x * blockDim.x) >> 5) {
+    const CrcBlock blk = blocks[b];
+    uint32_t per = (blk.len + 31) / 32;
+    per = (per + 7) & ~7u;
+    uint64_t s = (uint64_t)lane * per, e = s + per;
+    if (s > blk.len) s = blk.len;
+    if (e > blk.len) e = blk.len;
+    const uint8_t* p = out + blk.off;
+    uint32_t c = 0xFFFFFFFFu;
+    uint64_t i = s;
+    // align to 8 bytes of the absolute address
+    while (i < e && ((blk.off + i) & 7)) c = (c >> 8) ^ tab[0][(c ^ p[i++]) & 0xFF];
+    for (; i + 8 <= e; i += 8) {
+      uint2 w = *reinterpret_cast<const uint2*>(p + i);
+      uint32_t lo = w.x ^ c, hi = w.y;
+      c = tab[7][lo & 0xFF] ^ tab[6][(lo >> 8) & 0xFF] ^ tab[5][(lo >> 16) & 0xFF] ^
+          tab[4][lo >> 24] ^ tab[3][hi & 0xFF] ^ tab[2][(hi >> 8) & 0xFF] ^
+          tab[1][(hi >> 16) & 0xFF] ^ tab[0][hi >> 24];
+    }
+    while (i < e) c = (c >> 8) ^ tab[0][(c ^ p[i++]) & 0xFF];
+    c = ~c;
+    uint64_t len = e - s;
+    // tree combine across lanes, left to right
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      uint32_t c2 = __shfl_down_sync(0xFFFFFFFFu, c, d);
+      uint64_t l2 = __shfl_down_sync(0xFFFFFFFFu, len, d);
+      if ((lane & (2 * d - 1)) == 0 && lane + d < 32) {
+        c = crc_combine(c, c2, l2);
+        len += l2;
+      }
+    }
+    if (lane == 0) crcs[b] = c;
+  }
+}
+
+// one CTA per member: combine its block CRCs in order, check the trailer
+__global__ void crc_members_kernel(const CrcBlock* __restrict__ blocks,
+                                   const uint32_t* __restrict__ block_crcs,
+                                   const uint32_t* __restrict__ mem_block_begin,
+                                   const uint64_t* __restrict__ mem_trailer,
+                                   const uint64_t* __restrict__ mem_len, uint32_t n_mem,
+                                   const uint8_t* __restrict__ in, uint32_t* __restrict__ mem_crc,
+                                   int32_t* __restrict__ mem_status) {
+  __shared__ uint32_t sc[256];
+  __shared__ uint64_t sl[256];
+  uint32_t m = blockIdx.x;
+  if (m >= n_mem) return;
+  uint32_t b0 = mem_block_begin[m], b1 = mem_block_begin[m + 1];
+  uint32_t nb = b1 - b0;
+  // each thread folds a contiguous run of blocks
+  uint32_t per = (nb + blockDim.x - 1) / blockDim.x;
+  uint32_t s = threadIdx.x * per, e = min(s + per, nb);
+  uint32_t c = 0;
+  uint64_t len = 0;
+  for (uint32_t i = s; i < e; i++) {
+    c = len == 0 ? block_crcs[b0 + i] : crc_combine(c, block_crcs[b0 + i], blocks[b0 + i].len);
+    len += blocks[b0 + i].len;
+  }
+  sc[threadIdx.x] = c;
+  sl[threadIdx.x] = len;
+  __syncthreads();
+  for (int d = 1; d < (int)blockDim.x; d <<= 1) {
+    uint32_t cc = 0;
+    uint64_t ll = 0;
+    bool act = (threadIdx.x & (2 * d - 1)) == 0 && threadIdx.x + d < blockDim.x;
+    if (act) {
+      uint32_t c2 = sc[threadIdx.x + d];
+      uint64_t l2 = sl[threadIdx.x + d];
+      cc = sl[threadIdx.x] == 0 ? c2 : (l2 == 0 ? sc[threadIdx.x] : crc_combine(sc[threadIdx.x], c2, l2));
+      ll = sl[threadIdx.x] + l2;
+    }
+    __syncthreads();
+    if (act) {
+      sc[threadIdx.x] = cc;
+      sl[threadIdx.x] = ll;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    uint32_t crc = sc[0];
+    mem_crc[m] = crc;
+    uint64_t t = mem_trailer[m];
+    uint32_t ecrc = in[t] | (in[t + 1] << 8) | ((uint32_t)in[t + 2] << 16) | ((uint32_t)in[t + 3] << 24);
+    uint32_t eisz = in[t + 4] | (in[t + 5] << 8) | ((uint32_t)in[t + 6] << 16) | ((uint32_t)in[t + 7] << 24);
+    int32_t st = kOk;
+    if ((uint32_t)mem_len[m] != eisz) st = kSizeMismatch;
+    else if (crc != ecrc) st = kCrcMismatch;
+    mem_status[m] = st;
+  }
+}
+
+cudaError_t resolve_init(cudaStream_t stream) {
+  crc_init_kernel<<<1, 256, 0, stream>>>();
+  return cudaGetLastError();
+}
+
+cudaError_t launch_tail_literals(const PlacedChunk* placed, uint32_t n, const ChunkResult* results,
+                                 const PagePool& pool, uint8_t* out, cudaStream_t stream) {
+  if (!n) return cudaSuccess;
+  tail_literals_kernel<<<n, 256, 0, stream>>>(placed, n, results, pool, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_tail_markers(const PlacedChunk* placed, const uint32_t* list,
+                                const uint32_t* seg_begin, uint32_t n_seg,
+                                const ChunkResult* results, const PagePool& pool, uint8_t* out,
+                                cudaStream_t stream) {
+  if (!n_seg) return cudaSuccess;
+  tail_markers_kernel<<<n_seg, 1024, 0, stream>>>(placed, list, seg_begin, n_seg, results, pool,
+                                                   out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_body(const PlacedChunk* placed, const uint32_t* placed_of_chunk,
+                        uint32_t n_pages, const ChunkResult* results, const PagePool& pool,
+                        uint8_t* out, int sms, cudaStream_t stream) {
+  if (!n_pages) return cudaSuccess;
+  uint32_t blocks = n_pages < (uint32_t)(sms * 8) ? n_pages : (uint32_t)(sms * 8);
+  body_kernel<<<blocks, 512, 0, stream>>>(placed, placed_of_chunk, n_pages, results, pool, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_crc(const CrcBlock* blocks, uint32_t n_blocks, const uint8_t* out,
+                       uint32_t* block_crcs, const uint32_t* mem_block_begin,
+                       const uint64_t* mem_trailer, const uint64_t* mem_len, uint32_t n_mem,
+                       const uint8_t* in, uint32_t* mem_crc, int32_t* mem_status, int sms,
+                       cudaStream_t stream) {
+  if (n_blocks) {
+    uint32_t warps = n_blocks;
+    uint32_t blocks_needed = (warps + 7) / 8;
+    uint32_t grid = blocks_needed < (uint32_t)(sms * 8) ? blocks_needed : (uint32_t)(sms * 8);
+    crc_blocks_kernel<<<grid, 256, 0, stream>>>(blocks, n_blocks, out, block_crcs);
+  }
+  if (n_mem) {
+    crc_members_kernel<<<n_mem, 256, 0, stream>>>(blocks, block_crcs, mem_block_begin, mem_trailer,
+                                                   mem_len, n_mem, in, mem_crc, mem_status);
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace gzgpu

@@ -1,0 +1,137 @@
+/*
+ * gzgpu.h -- C ABI of the B200 gzip decompression backend.
+ *
+ * Drop-in for the decompression path of gzippy (JackDanger/gzippy v0.8.0).
+ * Each entry point names the reference interface it replaces (paths are
+ * relative to the reference project root).  Plain pointers and sizes only.
+ *
+ * Stream semantics follow the reference: input that does not start with
+ * the gzip magic 1f 8b yields GZGPU_NOT_GZIP and no output (the reference's
+ * Ok(empty), src/lib.rs:50-52); members are decoded in order and every
+ * member's CRC32 and ISIZE are verified; bytes after a member that do not
+ * start another gzip header end the stream cleanly; corrupt or truncated
+ * members are errors (src/decompress/mod.rs:742-870, tests/lib_api.rs:361-390).
+ *
+ * Threading: a context serialises its own calls (internal mutex); use one
+ * context per host thread for concurrency.  All host buffers belong to the
+ * caller; device buffers belong to the context.
+ */
+#ifndef GZGPU_H
+#define GZGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  The Rust shim maps GZGPU_NOT_GZIP to Ok(empty) and every
+ * other non-zero code to GzippyError::Decompression(gzgpu_strerror(code))
+ * (src/error.rs:7-46). */
+#define GZGPU_OK 0
+#define GZGPU_NOT_GZIP 1
+#define GZGPU_BAD_HEADER 2
+#define GZGPU_BAD_DEFLATE 3
+#define GZGPU_CRC_MISMATCH 4
+#define GZGPU_SIZE_MISMATCH 5
+#define GZGPU_OUT_TOO_SMALL 6 /* *out_len holds the size needed */
+#define GZGPU_DEVICE_ERROR 7
+#define GZGPU_TIMEOUT 8
+#define GZGPU_TRUNCATED 9
+#define GZGPU_INVALID_ARGUMENT 12
+
+/* readable bytes the device-resident entry point needs after the input */
+#define GZGPU_INPUT_PAD 1024
+
+typedef struct gzgpu_ctx gzgpu_ctx;
+
+typedef struct {
+  int device;         /* CUDA device ordinal */
+  size_t chunk_bytes; /* compressed bytes per speculative chunk; 0 = tuned default */
+  int lut_bits;       /* litlen LUT index bits: 10, 11 or 12; 0 = tuned default */
+  int autotune;       /* 1 = choose chunk_bytes / lut_bits per job from the tuning table */
+} gzgpu_config;
+
+typedef struct {
+  const uint8_t *data;
+  size_t len;
+} gzgpu_span;
+
+typedef struct {
+  uint8_t *data; /* caller buffer */
+  size_t cap;
+  size_t len;    /* set by the call: bytes written, or bytes needed (OUT_TOO_SMALL) */
+} gzgpu_out;
+
+typedef struct {
+  double ms_total;      /* device time of the last call (CUDA events) */
+  double ms_h2d, ms_scan, ms_find, ms_decode, ms_walk, ms_resolve, ms_crc, ms_d2h;
+  double ms_decode_kernel; /* the persistent inflate kernel alone (all passes) */
+  uint64_t in_bytes, out_bytes;
+  uint64_t n_streams, n_members, n_chunks, n_accepted, n_rejected, n_repairs;
+  uint64_t n_tail_marker_chunks, n_pages, decode_passes, kernel_launches;
+  uint64_t chunk_bytes;
+  int32_t lut_bits;
+  int32_t pad;
+} gzgpu_stats;
+
+/* Create / destroy a context on cfg->device (NULL cfg = defaults). */
+int gzgpu_create(gzgpu_ctx **out, const gzgpu_config *cfg);
+void gzgpu_destroy(gzgpu_ctx *ctx);
+const char *gzgpu_strerror(int code);
+
+/* gzippy::decompress / decompress_with_threads (src/lib.rs:176,189):
+ * host in -> host out.  The thread count of the reference has no meaning on
+ * the device and is not taken.  On GZGPU_OUT_TOO_SMALL *out_len is the
+ * size needed. */
+int gzgpu_decompress(gzgpu_ctx *ctx, const uint8_t *in, size_t in_len, uint8_t *out,
+                     size_t out_cap, size_t *out_len);
+
+/* gzippy::decompress_to_writer / _with_threads (src/lib.rs:204,221):
+ * output delivered in order through `write` (return 0 to continue, non-zero
+ * to abort with GZGPU_INVALID_ARGUMENT); *written = total bytes delivered. */
+typedef int (*gzgpu_write_fn)(void *user, const uint8_t *data, size_t len);
+int gzgpu_decompress_to_writer(gzgpu_ctx *ctx, const uint8_t *in, size_t in_len,
+                               gzgpu_write_fn write, void *user, uint64_t *written);
+
+/* Device-resident form of gzgpu_decompress (internal decompress_bytes,
+ * src/decompress/mod.rs:317): d_in / d_out are device pointers of this
+ * context's device, both 16-byte aligned (cudaMalloc memory is); d_in must
+ * have GZGPU_INPUT_PAD readable bytes past in_len.  No host copies of
+ * payload. */
+int gzgpu_decompress_device(gzgpu_ctx *ctx, const void *d_in, size_t in_len, void *d_out,
+                            size_t out_cap, size_t *out_len);
+
+/* Many independent streams in one job (no reference counterpart: the
+ * reference decodes one stream per call).  statuses[i] / outs[i].len per
+ * stream; returns GZGPU_OK when every stream decoded (or was not gzip). */
+int gzgpu_decompress_batch(gzgpu_ctx *ctx, const gzgpu_span *ins, size_t n, gzgpu_out *outs,
+                           int *statuses);
+
+/* Diagnostics (no reference counterpart; used by the parity tests).
+ *
+ * gzgpu_debug_find: run the block-finder kernel on `in` for n ranges
+ * [from[i], to[i]) (bit offsets); lo/hi = first candidate's (bit_offset,
+ * seek_bit), valid[i] = 0 when the range holds none.  Mirrors
+ * DeflateBlockValidator::find_first_candidate
+ * (src/decompress/parallel/blockfinder_validation.rs:319).
+ *
+ * gzgpu_debug_decode: run the inflate kernel on n explicit chunks (start
+ * bit, stop bit, member_first = zero window instead of markers) and copy
+ * each chunk's u16 entries to entries + i*cap_per.  res[6*i..] = end_bit,
+ * out_len, marker_end, n_blocks, status, final_block.  Mirrors
+ * decode_chunk (src/decompress/parallel/chunk_decode.rs:225). */
+int gzgpu_debug_find(gzgpu_ctx *ctx, const uint8_t *in, size_t in_len, const uint64_t *from,
+                     const uint64_t *to, size_t n, uint64_t *lo, uint64_t *hi, int *valid);
+int gzgpu_debug_decode(gzgpu_ctx *ctx, const uint8_t *in, size_t in_len, const uint64_t *start,
+                       const uint64_t *stop, const int *member_first, size_t n, uint16_t *entries,
+                       size_t cap_per, uint64_t *res);
+
+/* Statistics of the last call. */
+int gzgpu_get_stats(gzgpu_ctx *ctx, gzgpu_stats *out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GZGPU_H */

@@ -1,0 +1,192 @@
+"""GPU parity: the CUDA path (through the C ABI) against the oracle.
+
+Integer/byte work, so every comparison is bit-exact.  Kernel-level checks
+compare the finder's candidate and each chunk's u16 entries (markers
+included) with the oracle on the same inputs; end-to-end checks compare
+whole streams with the oracle and with zlib."""
+import io
+import zlib
+
+import numpy as np
+import pytest
+
+from oracle import pyoracle as O
+from gzippy_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def G():
+    import gzippy_b200 as G
+    return G
+
+
+@pytest.fixture(scope="module")
+def ctx(G):
+    c = G.Context(chunk_bytes=32 << 10)
+    yield c
+    c.close()
+
+
+def _stream(ctype, level, n, seed=1):
+    p = W.content(ctype, seed, n)
+    return p, W.gzip_member(p, level)
+
+
+@pytest.mark.parametrize("ctype", [W.MARKOV, W.RANDOM, W.RUNS, W.RAMPS])
+@pytest.mark.parametrize("level", [1, 6, 9])
+def test_stream_matches_oracle_and_zlib(ctx, ctype, level):
+    p, c = _stream(ctype, level, 700_000, seed=ctype * 10 + level)
+    got = ctx.decompress(c)
+    st, ref = O.decompress(c)
+    assert st == O.OK
+    assert got == ref.tobytes() == p.tobytes() == zlib.decompress(c.tobytes(), 31)
+
+
+def test_finder_matches_oracle(ctx):
+    p, c = _stream(W.MARKOV, 6, 2 << 20, seed=3)
+    p2, c2 = _stream(W.RANDOM, 6, 1 << 20, seed=4)
+    for data in (c, c2, np.concatenate([c, c2])):
+        nbits = data.size * 8
+        ranges = [(f, min(f + 64 * 1024 * 8, nbits)) for f in range(80, nbits, 97 * 1024 * 8 + 13)]
+        got = ctx.debug_find(data, ranges)
+        for (f, t), g in zip(ranges, got):
+            first, seek = O.find_blocks(data, f, t, cap=1 << 18)
+            exp = (int(first[0]), int(seek[0])) if first.size else None
+            assert g == exp, (f, t, g, exp)
+
+
+def test_decode_chunks_match_oracle(ctx):
+    """Window-absent chunks from finder starts: entries, markers, end bits."""
+    parts = [W.content(t, 5 + t, 1 << 20) for t in range(4)]
+    plain = np.concatenate(parts)
+    c = W.gzip_member(plain, 6)
+    _, hl = O.gzip_header_len(c)
+    nbits = c.size * 8
+    starts, step = [], 40 * 1024 * 8
+    for g in range(hl * 8 + step, nbits - 1000, step):
+        first, seek = O.find_blocks(c, g, min(g + step, nbits), cap=4)
+        if first.size:
+            starts.append((int(first[0]), int(seek[0])))
+    chunks = [(hl * 8, starts[0][0], True)]
+    for k, (lo, hi) in enumerate(starts):
+        stop = starts[k + 1][0] if k + 1 < len(starts) else 2**64 - 1
+        chunks.append((hi, stop, False))
+    cap = 4 << 20
+    res, ent = ctx.debug_decode(c, chunks, cap)
+    for i, (s, stop, mf) in enumerate(chunks):
+        st, r, e = O.inflate_chunk(c, s, stop, markers=not mf, cap=cap)
+        assert int(res[i, 4]) == st, i
+        if st != O.OK:
+            continue  # where an error is noticed is unspecified; the status must agree
+        assert int(res[i, 0]) == r.end_bit and int(res[i, 1]) == r.out_len
+        assert int(res[i, 2]) == r.marker_end and int(res[i, 5]) == r.final_block
+        assert int(res[i, 3]) == r.n_blocks
+        assert np.array_equal(ent[i, :r.out_len], e), i
+
+
+def test_single_member_chunked_pipeline(G):
+    parts = [W.content(t % 4, 100 + t, 1 << 20) for t in range(12)]
+    plain = np.concatenate(parts)
+    c = W.gzip_member(plain, 6, threads=4)
+    for cb in (16 << 10, 64 << 10, 1 << 20):
+        ctx = G.Context(chunk_bytes=cb)
+        got = ctx.decompress(c)
+        s = ctx.stats()
+        ctx.close()
+        assert got == plain.tobytes(), cb
+        assert s.n_accepted >= 1 and s.out_bytes == plain.size
+
+
+def test_level1_fixed_blocks_repair_path(G):
+    """No finder candidates inside fixed-Huffman data: the chain repairs."""
+    p = W.content(W.MARKOV, 8, 1 << 20)
+    c = W.gzip_member(p, 1)
+    ctx = G.Context(chunk_bytes=16 << 10)
+    assert ctx.decompress(c) == p.tobytes()
+    ctx.close()
+
+
+def test_multi_member(G, ctx):
+    plains, comps = [], []
+    for k in range(9):
+        p, c = _stream(k % 4, [1, 6, 9][k % 3], 50_000 + 37_000 * k, seed=k)
+        plains.append(p)
+        comps.append(c)
+    data = np.concatenate(comps)
+    assert ctx.decompress(data) == np.concatenate(plains).tobytes()
+
+
+def test_edge_cases(G, ctx):
+    p, c = _stream(W.MARKOV, 6, 100_000, seed=2)
+    cb = c.tobytes()
+    empty = zlib.compressobj(6, zlib.DEFLATED, 31)
+    e = empty.compress(b"") + empty.flush()
+    assert ctx.decompress(b"") == b""
+    assert ctx.decompress(b"\x1f") == b""
+    assert ctx.decompress(b"not gzip at all") == b""
+    assert ctx.decompress(e) == b""
+    assert ctx.decompress(e + cb) == p.tobytes()
+    assert ctx.decompress(cb + e + cb) == p.tobytes() * 2
+    assert ctx.decompress(cb + b"trailing garbage!!!!!") == p.tobytes()
+    tiny = zlib.compressobj(9, zlib.DEFLATED, 31)
+    t = tiny.compress(b"a") + tiny.flush()
+    assert ctx.decompress(t) == b"a"
+    with pytest.raises(G.GzippyError):
+        ctx.decompress(cb[:-30])
+    bad = bytearray(cb)
+    bad[-8] ^= 0x40
+    with pytest.raises(G.GzippyError) as ei:
+        ctx.decompress(bytes(bad))
+    assert ei.value.code == G.CRC_MISMATCH
+    bad = bytearray(cb)
+    bad[-2] ^= 1
+    with pytest.raises(G.GzippyError) as ei:
+        ctx.decompress(bytes(bad))
+    assert ei.value.code == G.SIZE_MISMATCH
+    bad = bytearray(cb)
+    bad[len(cb) // 2] ^= 0xFF
+    with pytest.raises(G.GzippyError):
+        ctx.decompress(bytes(bad))
+
+
+def test_header_fields(G, ctx):
+    """FTEXT/FHCRC/FEXTRA/FNAME/FCOMMENT members (RFC 1952 2.3.1)."""
+    p = W.content(W.RAMPS, 4, 200_000).tobytes()
+    raw = zlib.compressobj(6, zlib.DEFLATED, -15)
+    body = raw.compress(p) + raw.flush()
+    trailer = zlib.crc32(p).to_bytes(4, "little") + len(p).to_bytes(4, "little")
+    hdr = bytes([0x1f, 0x8b, 8, 0x1f, 0, 0, 0, 0, 0, 3]) + (6).to_bytes(2, "little") + b"XYZ\x00\x01\x02"
+    hdr += b"name.txt\x00" + b"a comment\x00"
+    hdr += (zlib.crc32(hdr) & 0xFFFF).to_bytes(2, "little")
+    data = hdr + body + trailer
+    assert ctx.decompress(data) == p
+    assert O.decompress(data)[1].tobytes() == p
+
+
+def test_writer_api(G, ctx):
+    p, c = _stream(W.RUNS, 6, 3 << 20, seed=7)
+    buf = io.BytesIO()
+    n = ctx.decompress_to_writer(c, buf)
+    assert n == p.size and buf.getvalue() == p.tobytes()
+    assert G.decompress_to_writer(b"xx", io.BytesIO()) == 0
+
+
+def test_batch_matches_individual(G, ctx):
+    rng = np.random.default_rng(0)
+    datas, plains = [], []
+    for i in range(60):
+        n = int(rng.integers(0, 300_000))
+        p, c = _stream(int(rng.integers(0, 4)), int(rng.choice([1, 6, 9])), n, seed=100 + i)
+        datas.append(c.tobytes())
+        plains.append(p.tobytes())
+    datas.append(b"not gzip")
+    plains.append(b"")
+    bad = bytearray(datas[3])
+    bad[-8] ^= 1
+    datas.append(bytes(bad))
+    res = ctx.decompress_batch(datas)
+    for i in range(61):
+        assert res[i] == plains[i], i
+    assert isinstance(res[61], G.GzippyError)
