@@ -1,0 +1,352 @@
+"""Decompressed-GB/s benchmark of the B200 gzip decode path.
+
+Workload (default): the single-member 1 GiB mixed stream -- 256 seeded 4 MiB
+segments cycling Markov text / uniform random / byte runs / uint16 ramps +
+noise, zlib level 6, one gzip member (generated on this machine; see
+gzippy_b200/workloads).  A step decodes the whole stream.
+
+  value : device-resident input -> device output (gzgpu_decompress_device),
+          GB/s of decompressed bytes; the K steps are bracketed by
+          synchronize + CUDA events on both sides, max over ranks.
+  e2e   : the reference-facing host call (gzgpu_decompress) with pinned host
+          buffers: H2D of the compressed stream and D2H of the output inside.
+  roofline : the inflate kernel, algorithmic bytes (compressed read +
+          decompressed written) per launch over its CUDA-event duration,
+          against the measured HBM copy bandwidth.
+
+`--impl reference` times the oracle's chunked speculative decoder (the C
+restatement of the reference's parallel single-member path) on all host
+threads, on the same workload.  Multi-GPU (torchrun): every rank decodes its
+own replica (weak scaling, no collective on the data path).
+"""
+from __future__ import annotations
+
+import argparse
+import hashlib
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "byte-exact decompressed GB/s on 1 B200, batched vs plain GPU path; p50/p99 ms"
+CACHE = os.path.join(tempfile.gettempdir(), "gzippy_b200_bench")
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def cpus() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def load_workload(name: str, scale: float):
+    """(compressed uint8 array, plain size, plain sha256, meta) -- cached on disk."""
+    from gzippy_b200 import workloads as W
+    os.makedirs(CACHE, exist_ok=True)
+    key = f"{name}_{scale:g}"
+    path = os.path.join(CACHE, key + ".gz")
+    meta_path = os.path.join(CACHE, key + ".json")
+    if os.path.exists(path) and os.path.exists(meta_path):
+        meta = json.load(open(meta_path))
+        return np.fromfile(path, dtype=np.uint8), meta
+    t0 = time.time()
+    if name == "single_member_mixed":
+        segs = max(4, int(round(256 * scale)))
+        wl = W.single_member_mixed(segments=segs, keep_plain=True)
+    elif name == "single_member_text":
+        wl = W.single_member_text(size=max(1 << 20, int((64 << 20) * scale)), keep_plain=True)
+    elif name == "multi_member":
+        wl = W.multi_member(members=max(8, int(2048 * scale)), keep_plain=True)
+    else:
+        raise SystemExit(f"unknown workload {name}")
+    comp = wl.compressed[0]
+    plain = wl.plain[0]
+    meta = {"name": name, "plain_bytes": int(plain.size), "comp_bytes": int(comp.size),
+            "sha256": hashlib.sha256(plain.tobytes()).hexdigest(),
+            "gen_s": round(time.time() - t0, 2), "meta": {k: v for k, v in wl.meta.items()
+                                                          if not isinstance(v, list)}}
+    comp.tofile(path)
+    json.dump(meta, open(meta_path, "w"))
+    return comp, meta
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.p:
+            self.p.terminate()
+            try:
+                self.p.wait(5)
+            except Exception:
+                self.p.kill()
+
+    def summary(self) -> dict:
+        self.f.flush()
+        rows = []
+        for line in open(self.f.name):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append((float(parts[1]), float(parts[2]), parts[5:9]))
+            except ValueError:
+                continue
+        os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for _, _, r in rows for i, v in enumerate(r) if v == "Active"})
+        return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows),
+                "reasons": reasons, "samples": len(rows)}
+
+
+def roofline_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        return float(json.load(open(p))["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def committed_traffic(workload: str):
+    """DRAM bytes per compressed byte of the inflate kernel from the committed
+    ncu summary (profiles/inflate_traffic.json), if any."""
+    p = os.path.join(ROOT, "profiles", "inflate_traffic.json")
+    if not os.path.exists(p):
+        return None
+    d = json.load(open(p))
+    return d.get("dram_bytes_per_comp_byte")
+
+
+def cpu_baseline(comp: np.ndarray, meta: dict, budget_s: float = 12.0, threads: int | None = None):
+    """The oracle's chunked speculative decoder on all host threads."""
+    from oracle import pyoracle as O
+    th = threads or cpus()
+    cap = meta["plain_bytes"] + 4096
+    st, out, _ = O.decompress_chunked(comp, chunk_bytes=4 << 20, threads=th, cap=cap)
+    assert st == O.OK and out.size == meta["plain_bytes"]
+    times, t_end = [], time.time() + budget_s
+    while time.time() < t_end or len(times) < 1:
+        t0 = time.perf_counter()
+        st, out, _ = O.decompress_chunked(comp, chunk_bytes=4 << 20, threads=th, cap=cap)
+        times.append(time.perf_counter() - t0)
+        if len(times) >= 20:
+            break
+    gbs = meta["plain_bytes"] / statistics.median(times) / 1e9
+    return {"value": round(gbs, 3), "unit": "GB/s", "cores": th, "kind": "port",
+            "sample": f"{len(times)} full decodes of the {meta['plain_bytes'] >> 20} MiB stream "
+                      f"(oracle chunked decoder, 4 MiB chunks, median)"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="single_member_mixed")
+    ap.add_argument("--scale", type=float, default=1.0)
+    ap.add_argument("--chunk-bytes", type=int, default=0)
+    ap.add_argument("--lut-bits", type=int, default=0)
+    ap.add_argument("--e2e-steps", type=int, default=0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.warmup < 3:
+        log("warmup raised to 3 (timing rule)")
+        args.warmup = 3
+
+    config = {"workload": args.workload, "streams": 1, "level": 6, "seed": 1235,
+              "plain_bytes": None, "comp_bytes": None,
+              "l2": "inputs (compressed) and outputs larger than the 126 MB L2; no flush",
+              "parallelism": f"replicas x{world}"}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        comp, meta = load_workload(args.workload, args.scale)
+        config.update(plain_bytes=meta["plain_bytes"], comp_bytes=meta["comp_bytes"])
+        th = cpus()
+        from oracle import pyoracle as O
+        cap = meta["plain_bytes"] + 4096
+        for _ in range(max(1, min(args.warmup, 1))):
+            st, out, _ = O.decompress_chunked(comp, chunk_bytes=4 << 20, threads=th, cap=cap)
+            assert st == O.OK and out.size == meta["plain_bytes"]
+        times = []
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            st, out, _ = O.decompress_chunked(comp, chunk_bytes=4 << 20, threads=th, cap=cap)
+            times.append(time.perf_counter() - t0)
+        ok = hashlib.sha256(out.tobytes()).hexdigest() == meta["sha256"]
+        sec = sum(times)
+        v = args.steps * meta["plain_bytes"] / sec / 1e9
+        line = {"metric": METRIC, "value": round(v, 4), "unit": "GB/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": round(1000 * sec / args.steps, 3), "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+                "data": "synthetic (seeded generator + zlib level 6)", "config": config,
+                "impl": "reference", "byte_exact": ok,
+                "cpu_baseline": {"value": round(v, 4), "unit": "GB/s", "cores": th, "kind": "port",
+                                 "sample": f"{args.steps} full decodes of the whole stream by the "
+                                           "oracle's chunked speculative decoder (4 MiB chunks)"},
+                "e2e": {"value": round(v, 4), "unit": "GB/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+
+    import torch
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    torch.cuda.set_device(local)
+    import gzippy_b200 as G
+    comp, meta = load_workload(args.workload, args.scale)
+    config.update(plain_bytes=meta["plain_bytes"], comp_bytes=meta["comp_bytes"])
+    ctx = G.Context(device=local, chunk_bytes=args.chunk_bytes, lut_bits=args.lut_bits)
+
+    # device-resident buffers (torch only allocates device memory here)
+    pad = 1024
+    d_in = torch.zeros(comp.size + pad, dtype=torch.uint8, device="cuda")
+    d_in[:comp.size].copy_(torch.from_numpy(comp))
+    d_out = torch.empty(meta["plain_bytes"] + 4096, dtype=torch.uint8, device="cuda")
+    torch.cuda.synchronize()
+
+    def step():
+        return ctx.decompress_device(d_in.data_ptr(), comp.size, d_out.data_ptr(), d_out.numel())
+
+    for _ in range(args.warmup):
+        n = step()
+    assert n == meta["plain_bytes"], (n, meta["plain_bytes"])
+    digest = hashlib.sha256(d_out[:n].cpu().numpy().tobytes()).hexdigest()
+    byte_exact = digest == meta["sha256"]
+    assert byte_exact, "device output differs from the plaintext"
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    # ---- timed region: value --------------------------------------------------
+    dec_ms, launches, st_last = [], 0, None
+    with ClockSampler(local) as clk:
+        barrier()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            step()
+            s = ctx.stats()
+            dec_ms.append(s.ms_decode_kernel)
+            launches += s.kernel_launches
+            st_last = s
+        e1.record()
+        torch.cuda.synchronize()
+        barrier()
+    ms = e0.elapsed_time(e1)
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * args.steps * meta["plain_bytes"] / (ms / 1e3) / 1e9
+    clocks = clk.summary()
+
+    # ---- e2e through the host C-ABI call with pinned buffers -------------------
+    e2e_steps = args.e2e_steps or max(1, min(args.steps, 3))
+    h_in = torch.from_numpy(comp).pin_memory()
+    h_out = torch.empty(meta["plain_bytes"] + 4096, dtype=torch.uint8).pin_memory()
+    hin_np, hout_np = h_in.numpy(), h_out.numpy()
+    n = ctx.decompress_into(hin_np, hout_np)
+    assert n == meta["plain_bytes"]
+    barrier()
+    torch.cuda.synchronize()
+    f0 = torch.cuda.Event(enable_timing=True)
+    f1 = torch.cuda.Event(enable_timing=True)
+    f0.record()
+    for _ in range(e2e_steps):
+        ctx.decompress_into(hin_np, hout_np)
+    f1.record()
+    torch.cuda.synchronize()
+    barrier()
+    e2e_ms = f0.elapsed_time(f1)
+    if dist is not None:
+        t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_ok = hashlib.sha256(hout_np[:n].tobytes()).hexdigest() == meta["sha256"]
+    e2e = {"value": round(world * e2e_steps * meta["plain_bytes"] / (e2e_ms / 1e3) / 1e9, 4),
+           "unit": "GB/s", "h2d_bytes_per_step": int(comp.size),
+           "d2h_bytes_per_step": int(meta["plain_bytes"]), "byte_exact": bool(e2e_ok)}
+
+    # ---- roofline of the inflate kernel --------------------------------------
+    peak, peak_kind = roofline_peak()
+    alg = comp.size + meta["plain_bytes"]       # compressed read once + bytes written once
+    kern_ms = statistics.mean(dec_ms)
+    achieved = alg / (kern_ms / 1e3) / 1e9
+    tpc = committed_traffic(args.workload)
+    roof = {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
+            "frac": round(achieved / peak, 5), "peak_kind": f"{peak_kind} (MEASURED_PEAKS hbm_gbs)",
+            "traffic": int(tpc * comp.size) if tpc else None,
+            "kernel": "inflate_kernel", "kernel_ms": round(kern_ms, 3),
+            "algorithmic_bytes": int(alg)}
+
+    line = {"metric": METRIC, "value": round(value, 4), "unit": "GB/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+            "data": "synthetic (seeded generator + zlib level 6)", "config": config,
+            "byte_exact": byte_exact, "e2e": e2e, "roofline": roof, "clocks": clocks,
+            "gpu_launches": int(launches),
+            "stages_ms": {k: round(getattr(st_last, k), 3) for k in
+                          ("ms_scan", "ms_find", "ms_decode", "ms_decode_kernel", "ms_walk",
+                           "ms_resolve", "ms_crc", "ms_total")},
+            "chunks": {"n": int(st_last.n_chunks), "accepted": int(st_last.n_accepted),
+                       "rejected": int(st_last.n_rejected), "repairs": int(st_last.n_repairs),
+                       "tail_marker_chunks": int(st_last.n_tail_marker_chunks),
+                       "chunk_bytes": int(st_last.chunk_bytes), "lut_bits": int(st_last.lut_bits)}}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(comp, meta)
+    ctx.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -46,7 +46,8 @@ class GzippyError(Exception):
 
 class Config(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("chunk_bytes", ctypes.c_size_t),
-                ("lut_bits", ctypes.c_int), ("autotune", ctypes.c_int)]
+                ("lut_bits", ctypes.c_int), ("autotune", ctypes.c_int),
+                ("ring_history", ctypes.c_int)]
 
 
 class Span(ctypes.Structure):
@@ -101,6 +102,7 @@ def lib():
             L.gzgpu_get_stats.argtypes = [vp, ctypes.POINTER(Stats)]
             L.gzgpu_debug_find.argtypes = [vp, vp, sz, vp, vp, sz, vp, vp, vp]
             L.gzgpu_debug_decode.argtypes = [vp, vp, sz, vp, vp, vp, sz, vp, sz, vp]
+            L.gzgpu_debug_last_chunks.argtypes = [vp, vp, vp, sz, ctypes.POINTER(sz)]
             _lib = L
     return _lib
 
@@ -127,9 +129,9 @@ class Context:
     """One device context (gzgpu_ctx): device buffers, stream, statistics."""
 
     def __init__(self, device: int = 0, chunk_bytes: int = 0, lut_bits: int = 0,
-                 autotune: bool = False):
+                 autotune: bool = False, ring_history: bool = False):
         self._lib = lib()
-        cfg = Config(device, chunk_bytes, lut_bits, int(autotune))
+        cfg = Config(device, chunk_bytes, lut_bits, int(autotune), int(ring_history))
         h = ctypes.c_void_p()
         rc = self._lib.gzgpu_create(ctypes.byref(h), ctypes.byref(cfg))
         if rc != OK:
@@ -254,6 +256,25 @@ class Context:
         if rc != OK:
             _raise(rc)
         return res, ent
+
+    DESC_DTYPE = np.dtype([("start_bit", "<u8"), ("lo_bit", "<u8"), ("stop_lo", "<u8"),
+                           ("guess_bit", "<u8"), ("limit_bit", "<u8"), ("in_end", "<u8"),
+                           ("abort_bit", "<u8"), ("flags", "<u4"), ("stream", "<u4")])
+    RESULT_DTYPE = np.dtype([("end_bit", "<u8"), ("out_len", "<u8"), ("marker_end", "<u8"),
+                             ("last_page", "<u4"), ("prev_page", "<u4"), ("n_pages", "<u4"),
+                             ("n_blocks", "<u4"), ("status", "<i4"), ("final_block", "<i4"),
+                             ("t_start", "<u8"), ("t_end", "<u8"), ("gen", "<u4"),
+                             ("pad", "<u4")])
+
+    def last_chunks(self):
+        """(descs, results) structured arrays of the last job's chunk table."""
+        n = ctypes.c_size_t(0)
+        self._lib.gzgpu_debug_last_chunks(self._h, None, None, 0, ctypes.byref(n))
+        d = np.zeros(n.value, self.DESC_DTYPE)
+        r = np.zeros(n.value, self.RESULT_DTYPE)
+        self._lib.gzgpu_debug_last_chunks(self._h, d.ctypes.data, r.ctypes.data, n.value,
+                                          ctypes.byref(n))
+        return d, r
 
     def decompress_batch(self, datas, caps=None):
         """Decode many streams in one job.  Returns a list of bytes (or a

@@ -36,6 +36,7 @@ enum : int32_t {
   kTruncated = 9,
   kPoolExhausted = 10,
   kNotDecoded = 11,
+  kOvershoot = 13,  // speculative chunk ran past stop_lo + slack without a block boundary
 };
 
 enum : uint32_t {
@@ -50,6 +51,7 @@ struct ChunkDesc {
   uint64_t guess_bit;  // partition start the finder searched from
   uint64_t limit_bit;  // end of the finder's search range
   uint64_t in_end;     // byte end of this chunk's stream in the input buffer
+  uint64_t abort_bit;  // a speculative chunk gives up past this bit (kNoStop = never)
   uint32_t flags;
   uint32_t stream;     // stream id
 };
@@ -64,7 +66,15 @@ struct ChunkResult {
   uint32_t n_blocks;
   int32_t status;
   int32_t final_block;
+  uint64_t t_start, t_end;  // %globaltimer (ns) when the warp took / finished the chunk
+  uint32_t gen;             // decode attempt that produced this result (page tag)
+  uint32_t pad;
 };
+
+// a page's seq word: attempt (gen) in the top 8 bits, page index below
+constexpr uint32_t kSeqMask = 0x00FFFFFFu;
+constexpr int kGenShift = 24;
+constexpr uint32_t kMaxTries = 4;  // speculative starts tried per chunk
 
 struct PagePool {
   uint16_t* data;    // cap * kPageEntries entries

@@ -120,7 +120,8 @@ const char* kErrStr[] = {"ok",
                          "truncated input",
                          "device page pool exhausted",
                          "chunk not decoded",
-                         "invalid argument"};
+                         "invalid argument",
+                         "speculative chunk overshot its stop"};
 
 }  // namespace
 
@@ -131,6 +132,7 @@ struct gzgpu_ctx {
   size_t chunk_bytes = 0;
   int lut_bits = 10;
   bool autotune = false;
+  bool ring = false;  // history layout of the inflate kernel (false = pages)
   int decode_blocks = 0;
   cudaEvent_t ev[12];
   gzgpu_stats stats{};
@@ -163,15 +165,15 @@ struct gzgpu_ctx {
     stats.decode_passes++;
     switch (lut_bits) {
       case 11:
-        return launch_inflate<11>(cur_in, descs.as<ChunkDesc>(), results.as<ChunkResult>(),
+        return launch_inflate<11>(ring, cur_in, descs.as<ChunkDesc>(), results.as<ChunkResult>(),
                                   work.as<uint32_t>(), d_work_count, counters.as<uint32_t>() + 3,
                                   pool, decode_blocks, st);
       case 12:
-        return launch_inflate<12>(cur_in, descs.as<ChunkDesc>(), results.as<ChunkResult>(),
+        return launch_inflate<12>(ring, cur_in, descs.as<ChunkDesc>(), results.as<ChunkResult>(),
                                   work.as<uint32_t>(), d_work_count, counters.as<uint32_t>() + 3,
                                   pool, decode_blocks, st);
       default:
-        return launch_inflate<10>(cur_in, descs.as<ChunkDesc>(), results.as<ChunkResult>(),
+        return launch_inflate<10>(ring, cur_in, descs.as<ChunkDesc>(), results.as<ChunkResult>(),
                                   work.as<uint32_t>(), d_work_count, counters.as<uint32_t>() + 3,
                                   pool, decode_blocks, st);
     }
@@ -180,9 +182,9 @@ struct gzgpu_ctx {
   int setup_decode_grid() {
     int per_sm = 1;
     switch (lut_bits) {
-      case 11: per_sm = inflate_blocks_per_sm<11>(); break;
-      case 12: per_sm = inflate_blocks_per_sm<12>(); break;
-      default: per_sm = inflate_blocks_per_sm<10>(); break;
+      case 11: per_sm = inflate_blocks_per_sm<11>(ring); break;
+      case 12: per_sm = inflate_blocks_per_sm<12>(ring); break;
+      default: per_sm = inflate_blocks_per_sm<10>(ring); break;
     }
     if (per_sm < 1) per_sm = 1;
     decode_blocks = per_sm * sms;
@@ -190,6 +192,10 @@ struct gzgpu_ctx {
   }
 
   int run(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R);
+
+  // chunk tables of the last job (diagnostics)
+  std::vector<ChunkDesc> last_descs;
+  std::vector<ChunkResult> last_results;
 };
 
 static uint64_t pick_chunk_bytes(uint64_t in_len) {
@@ -355,7 +361,8 @@ int gzgpu_ctx::run(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R) 
                                 (uint32_t)hspec.size(), st))))
     return rc;
   if ((rc = check(launch_link(descs.as<ChunkDesc>(), n_grid, work.as<uint32_t>(),
-                              counters.as<uint32_t>() + 1, st))))
+                              counters.as<uint32_t>() + 1, std::max<uint64_t>(cbits, 1ull << 21),
+                              st))))
     return rc;
   stats.kernel_launches += 2;
   cudaEventRecord(ev[4], st);
@@ -413,6 +420,7 @@ int gzgpu_ctx::run(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R) 
     d.start_bit = d.lo_bit = d.guess_bit = d.limit_bit = start;
     if (flags & kChunkMemberFirst) d.limit_bit = S[w.stream].off + w.mpos;
     d.stop_lo = stop;
+    d.abort_bit = kNoStop;
     d.in_end = S[w.stream].off + S[w.stream].len;
     d.flags = flags | kChunkValid;
     d.stream = w.stream;
@@ -518,12 +526,15 @@ int gzgpu_ctx::run(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R) 
         w.j = j + 1;
         continue;
       }
-      while (j < w.c1 && (!is_valid(j) || (!is_mf(j) && hd[j].lo_bit <= e))) {
+      // discard starts the confirmed end passed: speculative candidates and
+      // member candidates that lay inside this member's data
+      auto first_bit = [&](uint32_t k) { return is_mf(k) ? hd[k].limit_bit * 8 : hd[k].lo_bit; };
+      while (j < w.c1 && (!is_valid(j) || first_bit(j) <= e)) {
         if (is_valid(j)) n_rejected++;
         j++;
       }
       w.j = j;
-      uint64_t stop = (j < w.c1 && !is_mf(j)) ? hd[j].lo_bit : kNoStop;
+      uint64_t stop = j < w.c1 ? first_bit(j) : kNoStop;
       new_chunk(w, e, stop, 0);
       break;
     }
@@ -579,6 +590,8 @@ int gzgpu_ctx::run(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R) 
   }
   stats.n_rejected = n_rejected;
   stats.n_repairs = n_repairs;
+  last_descs = hd;
+  last_results = hr;
   // ---- output placement ----------------------------------------------------
   const uint32_t n_all = (uint32_t)hd.size();
   std::vector<PlacedChunk> placed;
@@ -734,6 +747,7 @@ int gzgpu_create(gzgpu_ctx** out, const gzgpu_config* cfg) {
     c->chunk_bytes = cfg->chunk_bytes;
     if (cfg->lut_bits == 11 || cfg->lut_bits == 12) c->lut_bits = cfg->lut_bits;
     c->autotune = cfg->autotune != 0;
+    c->ring = cfg->ring_history != 0;
   }
   if (cudaSetDevice(c->dev) != cudaSuccess) {
     delete c;
@@ -1026,6 +1040,7 @@ int gzgpu_debug_decode(gzgpu_ctx* c, const uint8_t* in, size_t in_len, const uin
     d[i] = ChunkDesc{};
     d[i].start_bit = d[i].lo_bit = d[i].guess_bit = d[i].limit_bit = start[i];
     d[i].stop_lo = stop[i];
+    d[i].abort_bit = kNoStop;
     d[i].in_end = in_len;
     d[i].flags = kChunkValid | (member_first[i] ? kChunkMemberFirst : 0u);
     wl[i] = (uint32_t)i;
@@ -1064,14 +1079,24 @@ int gzgpu_debug_decode(gzgpu_ctx* c, const uint8_t* in, size_t in_len, const uin
   if (entries) {
     for (uint32_t p = 0; p < used; p++) {
       uint32_t cid = own[p];
-      if (cid >= n || r[cid].status != kOk) continue;
-      uint64_t q0 = (uint64_t)sq[p] * kPageEntries;
+      if (cid >= n || r[cid].status != kOk || (sq[p] >> kGenShift) != r[cid].gen) continue;
+      uint64_t q0 = (uint64_t)(sq[p] & kSeqMask) * kPageEntries;
       if (q0 >= r[cid].out_len || q0 >= cap_per) continue;
       uint64_t k = std::min<uint64_t>({(uint64_t)kPageEntries, r[cid].out_len - q0, cap_per - q0});
       cudaMemcpy(entries + cid * cap_per + q0, c->pages.as<uint16_t>() + (size_t)p * kPageEntries,
                  2 * k, cudaMemcpyDeviceToHost);
     }
   }
+  return GZGPU_OK;
+}
+
+int gzgpu_debug_last_chunks(gzgpu_ctx* c, void* descs, void* results, size_t cap, size_t* n) {
+  if (!c || !n) return GZGPU_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> g(c->mu);
+  *n = c->last_descs.size();
+  size_t k = std::min(cap, c->last_descs.size());
+  if (descs && k) memcpy(descs, c->last_descs.data(), k * sizeof(ChunkDesc));
+  if (results && k) memcpy(results, c->last_results.data(), k * sizeof(ChunkResult));
   return GZGPU_OK;
 }
 

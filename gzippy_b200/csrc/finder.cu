@@ -1,153 +1,14 @@
 // finder.cu -- deflate block-boundary finder (K1) and chunk linking.
 //
 // One warp per speculative chunk searches [guess_bit, limit_bit) for the
-// first block-start candidate in (bit_offset, seek_bit) order, with the
-// reference's predicate (src/decompress/parallel/blockfinder_validation.rs):
-//   dynamic: BFINAL=0, BTYPE=10, HLIT<=29, HDIST<=29 (13-bit filter,
-//            :68-150); precode leaf count 128 or 64 (validate_precode
-//            :190-226) and Kraft-exact (is_valid_huffman_lengths :807-830);
-//            the HLIT+257+HDIST+1 code lengths decode with the precode,
-//            EOB has a code, litlen and dist sets are Kraft-exact
-//            (validate_huffman_codes :836-925).  No fixed-Huffman candidates.
-//   stored:  LEN == ~NLEN at a byte boundary preceded by 3 zero header bits;
-//            the candidate spans [byte_bit - zero_run, byte_bit - 3]
-//            (find_uncompressed_blocks :370-475).
-// Lanes test 32 byte offsets (stored) or 32 bit offsets (dynamic) per step;
-// a ballot picks the lowest hit.  The stored scan runs first so the dynamic
-// scan can stop at the first stored candidate.
+// first block-start candidate (predicate and search in finder_core.cuh).
 #include <cstdint>
 
 #include "common.cuh"
 #include "finder.cuh"
+#include "finder_core.cuh"
 
 namespace gzgpu {
-
-__constant__ uint8_t f_cl_order[19] = {16, 17, 18, 0, 8, 7, 9, 6, 10, 5, 11, 4, 12, 3, 13, 2, 14, 1, 15};
-
-// bits [bit, bit+k) of the input, k <= 57; bytes at or past `nbytes` read 0
-__device__ __forceinline__ uint64_t peek_bits(const uint8_t* in, uint64_t nbytes, uint64_t bit,
-                                              int k) {
-  uint64_t byte = bit >> 3;
-  uint64_t v = 0;
-#pragma unroll
-  for (int i = 0; i < 8; i++) {
-    uint64_t b = byte + i;
-    v |= (uint64_t)(b < nbytes ? in[b] : 0) << (8 * i);
-  }
-  return (v >> (bit & 7)) & ((1ull << k) - 1);
-}
-
-// Kraft equality over 15-bit leaves, or a single one-bit code.
-__device__ __forceinline__ bool kraft_exact(uint32_t leaves, uint32_t gt1) {
-  if (leaves == (1u << 14)) return gt1 == 0;
-  return leaves == (1u << 15);
-}
-
-// Full dynamic-header predicate at `bit`.  `base` = stream start byte,
-// `nbytes` = stream end byte (absolute).
-__device__ bool dyn_candidate(const uint8_t* in, uint64_t nbytes, uint64_t bit) {
-  const uint64_t nbits = nbytes * 8;
-  if (bit + 17 > nbits) return false;
-  uint32_t h = (uint32_t)peek_bits(in, nbytes, bit, 17);
-  if ((h & 1) || ((h >> 1) & 3) != 2 || ((h >> 3) & 31) > 29 || ((h >> 8) & 31) > 29) return false;
-  int hlit = (h >> 3) & 31, hdist = (h >> 8) & 31, pc = ((h >> 13) & 15) + 4;
-  if (bit + 17 + 3 * pc > nbits) return false;
-  uint64_t pbits = peek_bits(in, nbytes, bit + 17, 3 * pc);
-  uint32_t leaves7 = 0, leaves15 = 0, gt1 = 0;
-  uint8_t cl[19];
-#pragma unroll
-  for (int i = 0; i < 19; i++) cl[i] = 0;
-  for (int i = 0; i < pc; i++) {
-    uint32_t L = (uint32_t)(pbits >> (3 * i)) & 7;
-    cl[f_cl_order[i]] = (uint8_t)L;
-    if (L) {
-      leaves7 += 1u << (7 - L);
-      leaves15 += 1u << (15 - L);
-      gt1 += L > 1;
-    }
-  }
-  if (leaves7 != 128 && leaves7 != 64) return false;
-  if (!kraft_exact(leaves15, gt1)) return false;
-  // canonical precode tables
-  uint16_t cnt[8], first[8], offs[8];
-  uint8_t sorted[19];
-#pragma unroll
-  for (int L = 0; L < 8; L++) cnt[L] = 0;
-  for (int s = 0; s < 19; s++) cnt[cl[s]]++;
-  cnt[0] = 0;
-  {
-    uint32_t code = 0, off = 0;
-    for (int L = 1; L < 8; L++) {
-      if (L > 1) code = (code + cnt[L - 1]) << 1;
-      first[L] = (uint16_t)code;
-      offs[L] = (uint16_t)off;
-      off += cnt[L];
-    }
-    uint16_t nx[8];
-    for (int L = 0; L < 8; L++) nx[L] = offs[L];
-    for (int s = 0; s < 19; s++)
-      if (cl[s]) sorted[nx[cl[s]]++] = (uint8_t)s;
-  }
-  // decode the litlen + dist code lengths, accumulating Kraft sums
-  const int hl = 257 + hlit, total = hl + 1 + hdist;
-  uint64_t pos = bit + 17 + 3 * pc;
-  uint32_t lit_leaves = 0, lit_gt1 = 0, dist_leaves = 0, dist_gt1 = 0;
-  int i = 0;
-  uint32_t prev = 0, eob_len = 0;
-  while (i < total) {
-    if (pos >= nbits) return false;
-    uint32_t w = (uint32_t)peek_bits(in, nbytes, pos, 14);
-    // MSB-first 7-bit code
-    uint32_t rev = __brev(w) >> 25;
-    int sym = -1;
-    for (int L = 1; L < 8; L++) {
-      uint32_t c = rev >> (7 - L);
-      uint32_t idx = c - first[L];
-      if (idx < cnt[L]) {
-        sym = sorted[offs[L] + idx];
-        pos += L;
-        break;
-      }
-    }
-    if (sym < 0) return false;
-    uint32_t v;
-    int rep;
-    if (sym < 16) {
-      v = sym;
-      rep = 1;
-    } else if (sym == 16) {
-      if (i == 0) return false;
-      v = prev;
-      rep = 3 + (int)peek_bits(in, nbytes, pos, 2);
-      pos += 2;
-    } else if (sym == 17) {
-      v = 0;
-      rep = 3 + (int)peek_bits(in, nbytes, pos, 3);
-      pos += 3;
-    } else {
-      v = 0;
-      rep = 11 + (int)peek_bits(in, nbytes, pos, 7);
-      pos += 7;
-    }
-    if (i + rep > total) return false;
-    if (pos > nbits) return false;
-    if (v) {
-      int n_lit = i < hl ? min(rep, hl - i) : 0;
-      int n_dist = rep - n_lit;
-      lit_leaves += (uint32_t)n_lit << (15 - v);
-      dist_leaves += (uint32_t)n_dist << (15 - v);
-      if (v > 1) {
-        lit_gt1 += n_lit;
-        dist_gt1 += n_dist;
-      }
-      if (i <= 256 && 256 < i + rep) eob_len = v;
-    }
-    prev = v;
-    i += rep;
-  }
-  if (eob_len == 0) return false;
-  return kraft_exact(lit_leaves, lit_gt1) && kraft_exact(dist_leaves, dist_gt1);
-}
 
 __global__ void finder_kernel(const uint8_t* __restrict__ in, ChunkDesc* descs,
                               const uint32_t* __restrict__ spec, uint32_t n_spec) {
@@ -155,66 +16,12 @@ __global__ void finder_kernel(const uint8_t* __restrict__ in, ChunkDesc* descs,
   const uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (w >= n_spec) return;
   ChunkDesc& d = descs[spec[w]];
-  const uint64_t from = d.guess_bit, nbytes = d.in_end;
-  uint64_t to = d.limit_bit;
-  if (to > nbytes * 8) to = nbytes * 8;
-  bool have = false;
-  uint64_t best_lo = 0, best_hi = 0;
-  // stored candidates: first hit in byte order has the smallest bit_offset
-  if (nbytes >= 5) {
-    uint64_t until = (to + 7) / 8;
-    if (until > nbytes - 4) until = nbytes - 4;
-    uint64_t sb = (from + 3 + 7) / 8;
-    if (sb < 2) sb = 2;
-    for (uint64_t off0 = sb; off0 < until && !have; off0 += 32) {
-      uint64_t off = off0 + lane;
-      bool hit = false;
-      uint64_t lo = 0, hi = 0;
-      if (off < until) {
-        uint32_t sz = in[off] | (in[off + 1] << 8) | ((uint32_t)in[off + 2] << 16) |
-                      ((uint32_t)in[off + 3] << 24);
-        if (((sz ^ (sz >> 16)) & 0xFFFF) == 0xFFFF) {
-          uint64_t byte_bit = off * 8;
-          uint32_t pre = (uint32_t)peek_bits(in, nbytes, byte_bit - 10, 10);
-          if ((pre & (7u << 7)) == 0) {
-            int tz = 3;
-            for (int j = 4; j <= 10; j++) {
-              if (pre & (1u << (10 - j))) break;
-              tz = j;
-            }
-            lo = byte_bit - tz;
-            hi = byte_bit - 3;
-            uint32_t len = sz & 0xFFFF;
-            hit = lo >= from && hi < to && len != 0 && off + 4 + len <= nbytes;
-          }
-        }
-      }
-      uint32_t m = __ballot_sync(0xFFFFFFFFu, hit);
-      if (m) {
-        int src = __ffs(m) - 1;
-        best_lo = __shfl_sync(0xFFFFFFFFu, lo, src);
-        best_hi = __shfl_sync(0xFFFFFFFFu, hi, src);
-        have = true;
-      }
-    }
-  }
-  // dynamic candidates below the stored one (a tie at its bit_offset sorts first)
-  uint64_t lim = have ? best_lo + 1 : to;
-  for (uint64_t p0 = from; p0 < lim; p0 += 32) {
-    uint64_t p = p0 + lane;
-    bool hit = p < lim && dyn_candidate(in, nbytes, p);
-    uint32_t m = __ballot_sync(0xFFFFFFFFu, hit);
-    if (m) {
-      uint64_t q = p0 + (__ffs(m) - 1);
-      best_lo = best_hi = q;
-      have = true;
-      break;
-    }
-  }
+  uint64_t lo = 0, hi = 0;
+  bool have = warp_find_first(in, d.in_end, d.guess_bit, d.limit_bit, lane, lo, hi);
   if (lane == 0) {
     if (have) {
-      d.lo_bit = best_lo;
-      d.start_bit = best_hi;
+      d.lo_bit = lo;
+      d.start_bit = hi;
       d.flags |= kChunkValid;
     } else {
       d.flags &= ~kChunkValid;
@@ -225,7 +32,11 @@ __global__ void finder_kernel(const uint8_t* __restrict__ in, ChunkDesc* descs,
 // stop_lo of each valid chunk = lo of the next valid chunk when that one is
 // speculative (member starts end their predecessor at BFINAL instead);
 // valid chunks are appended to the decode work list.
-__global__ void link_kernel(ChunkDesc* descs, uint32_t n, uint32_t* work, uint32_t* n_work) {
+// A speculative start may be a phantom whose garbage code table never fails;
+// such a chunk gives up `slack` bits past its stop and the chain walk
+// re-decodes the gap from the confirmed boundary instead.
+__global__ void link_kernel(ChunkDesc* descs, uint32_t n, uint32_t* work, uint32_t* n_work,
+                            uint64_t slack) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   ChunkDesc& d = descs[i];
@@ -233,13 +44,20 @@ __global__ void link_kernel(ChunkDesc* descs, uint32_t n, uint32_t* work, uint32
   uint64_t stop = kNoStop;
   for (uint32_t j = i + 1; j < n; j++) {
     uint32_t f = descs[j].flags;
-    if (f & kChunkMemberFirst) break;
+    if (descs[j].stream != d.stream) break;
+    if (f & kChunkMemberFirst) {
+      // a member candidate (limit_bit = its header byte): a real one follows
+      // the BFINAL block, a false one lies inside this member's data
+      stop = descs[j].limit_bit * 8;
+      break;
+    }
     if (f & kChunkValid) {
       stop = descs[j].lo_bit;
       break;
     }
   }
   d.stop_lo = stop;
+  d.abort_bit = (stop != kNoStop && !(d.flags & kChunkMemberFirst)) ? stop + slack : kNoStop;
   work[atomicAdd(n_work, 1u)] = i;
 }
 
@@ -253,9 +71,9 @@ cudaError_t launch_finder(const uint8_t* in, ChunkDesc* descs, const uint32_t* s
 }
 
 cudaError_t launch_link(ChunkDesc* descs, uint32_t n, uint32_t* work, uint32_t* n_work,
-                        cudaStream_t stream) {
+                        uint64_t slack_bits, cudaStream_t stream) {
   if (n == 0) return cudaSuccess;
-  link_kernel<<<(n + 255) / 256, 256, 0, stream>>>(descs, n, work, n_work);
+  link_kernel<<<(n + 255) / 256, 256, 0, stream>>>(descs, n, work, n_work, slack_bits);
   return cudaGetLastError();
 }
 

@@ -9,6 +9,6 @@ namespace gzgpu {
 cudaError_t launch_finder(const uint8_t* in, ChunkDesc* descs, const uint32_t* spec,
                           uint32_t n_spec, cudaStream_t stream);
 cudaError_t launch_link(ChunkDesc* descs, uint32_t n, uint32_t* work, uint32_t* n_work,
-                        cudaStream_t stream);
+                        uint64_t slack_bits, cudaStream_t stream);
 
 }  // namespace gzgpu

@@ -1,22 +1,32 @@
 // inflate.cu -- speculative chunk inflate (RFC 1951) for sm_100a.
 //
 // One warp decodes one chunk.  All 32 lanes run the serial Huffman decode in
-// lock-step on identical state (so table reads are shared-memory broadcasts
-// and control flow never diverges); the lanes split the work that is
-// parallel: LZ77 copies (32 entries per step), stored-block copies, table
-// builds and ring -> page flushes (16-byte vector stores).
+// lock-step on identical state (table reads are shared-memory broadcasts and
+// control flow never diverges); the lanes split the work that is parallel:
+// LZ77 copies (32 entries per step), stored-block copies and table builds.
 //
-// History lives on chip: a 32 Ki-entry u16 ring in shared memory per warp.
-// A chunk that starts without a window pre-seeds the ring with marker values
-// (entry i = 32768 + i), so a back-reference that reaches before the chunk
-// copies the marker for the window byte it needs; copies of markers stay
-// markers.  This is the marker scheme of the reference
-// (src/decompress/parallel/marker_inflate.rs init_marker_zone :265,
-// replace_markers.rs:7-23).  A member's first chunk seeds zeros instead
-// (the zero window of chunk_fetcher.rs:696).
+// Entries are u16: a byte (< 256), or a window marker (>= 32768) for a
+// back-reference that reaches before the chunk into the unknown 32 KiB
+// window: window index w = 32768 + pos - dist gives the entry 32768 + w; a
+// copy of a marker stays a marker.  This is the marker scheme of the
+// reference (src/decompress/parallel/marker_inflate.rs init_marker_zone
+// :265, replace_markers.rs:7-23).  A member's first chunk reads zeros there
+// instead (the zero window of chunk_fetcher.rs:696).
+//
+// Two history layouts, same decode:
+//   pages (default) : the chunk writes its entries straight into its output
+//                     pages in HBM and reads back-references from them; a
+//                     warp keeps only its Huffman tables (~7 KB) in shared
+//                     memory, so an SM runs ~32 decoding warps and hides the
+//                     latency of the serial symbol chain across them.
+//   ring            : a 32 Ki-entry u16 ring per warp in shared memory
+//                     (64 KB), flushed to the pages in 8 Ki-entry units;
+//                     on-chip history, 3 decoding warps per SM.
 //
 // Stop rule (chunk_decode.rs decode_chunk :225): before each block header,
 // stop if the bit position is >= stop_lo; the BFINAL block ends the chunk.
+// A speculative chunk that fails moves on to its partition's next candidate
+// (chunk_fetcher.rs speculative_decode_find_boundary :2616-2740).
 //
 // Input bits come from a two-window register stage: every lane holds one
 // 32-bit word of the current and the next 128-byte input window; the bit
@@ -25,6 +35,7 @@
 #include <cstdint>
 
 #include "common.cuh"
+#include "finder_core.cuh"
 #include "inflate.cuh"
 
 namespace gzgpu {
@@ -61,20 +72,26 @@ __device__ __forceinline__ uint32_t dist_entry(uint32_t sym, uint32_t L) {
 }
 __device__ __forceinline__ uint32_t pre_entry(uint32_t sym, uint32_t L) { return (sym << 16) | L; }
 
+// Per-warp Huffman tables (shared memory).
 template <int LB>
-struct alignas(16) WarpSmem {
-  uint16_t ring[kWindow];       // decoded history (u16 entries)
+struct alignas(16) Tables {
   uint32_t lit_lut[1 << LB];
   uint32_t dist_lut[1 << kDistBits];
   uint32_t pre_lut[128];
   uint16_t lit_sorted[288];
   uint16_t dist_sorted[32];
-  uint16_t pre_sorted[19];
+  uint16_t pre_sorted[20];
   uint16_t lit_count[16], lit_first[16], lit_offs[16];
   uint16_t dist_count[16], dist_first[16], dist_offs[16];
   uint16_t pre_count[16], pre_first[16], pre_offs[16];
   uint16_t next[16];
   uint8_t lens[320];
+};
+
+template <int LB>
+struct alignas(16) RingSmem {
+  uint16_t ring[kWindow];
+  Tables<LB> t;
 };
 
 // ---------------------------------------------------------------------------
@@ -140,8 +157,8 @@ template <int TB, typename EntryFn>
 __device__ bool build_table(const uint8_t* lens, int n, uint16_t* count, uint16_t* first,
                             uint16_t* offs, uint16_t* sorted, uint16_t* next, uint32_t* lut,
                             int lane, EntryFn entry) {
-  // histogram by ballots (no shared atomics on 16-bit words)
-  uint32_t cnt_l = 0;  // lane l (1..15) accumulates count[l]
+  // histogram by ballots: lane L (1..15) accumulates count[L]
+  uint32_t cnt_l = 0;
   for (int g = 0; g < n; g += 32) {
     int s = g + lane;
     uint32_t l = s < n ? lens[s] : 0;
@@ -217,31 +234,192 @@ __device__ __forceinline__ uint32_t slow_decode(uint64_t bb, const uint16_t* cou
   return 0;
 }
 
+// Fixed (btype 1) or dynamic (btype 2) block tables; the 3 header bits are
+// already consumed.  Returns kOk or an error status.
+template <int LB>
+__device__ int32_t read_tables(BitReader& br, uint32_t btype, Tables<LB>* T, uint64_t trunc_words,
+                               int lane) {
+  bool ok;
+  if (btype == 1) {
+    // fixed Huffman (RFC 1951 3.2.6): litlen 0..287, then 32 distance codes
+    for (int s = lane; s < 320; s += 32) {
+      uint8_t l;
+      if (s < 144) l = 8;
+      else if (s < 256) l = 9;
+      else if (s < 280) l = 7;
+      else if (s < 288) l = 8;
+      else l = 5;
+      T->lens[s] = l;
+    }
+    __syncwarp();
+    ok = build_table<LB>(T->lens, 288, T->lit_count, T->lit_first, T->lit_offs, T->lit_sorted,
+                         T->next, T->lit_lut, lane, litlen_entry);
+    ok = ok && build_table<kDistBits>(T->lens + 288, 32, T->dist_count, T->dist_first,
+                                      T->dist_offs, T->dist_sorted, T->next, T->dist_lut, lane,
+                                      dist_entry);
+    return ok ? kOk : kBadDeflate;
+  }
+  // dynamic header (RFC 1951 3.2.7)
+  br.refill(lane);
+  uint32_t h = (uint32_t)br.bb & 0x3FFF;
+  br.consume(14);
+  int nlen = 257 + (h & 31), ndist = 1 + ((h >> 5) & 31), ncl = 4 + (h >> 10);
+  if (nlen > 286 || ndist > 30) return kBadDeflate;
+  // code-length code lengths: 3 bits each, read as up to 10 + 9
+  uint32_t clv = 0;
+  int n1 = ncl < 10 ? ncl : 10;
+  br.refill(lane);
+  if (lane < n1) clv = (uint32_t)(br.bb >> (3 * lane)) & 7;
+  br.consume(3 * n1);
+  br.refill(lane);
+  if (lane >= 10 && lane < ncl) clv = (uint32_t)(br.bb >> (3 * (lane - 10))) & 7;
+  br.consume(3 * (ncl - n1));
+  if (lane < 19) T->lens[296 + c_cl_order[lane]] = (uint8_t)clv;
+  __syncwarp();
+  ok = build_table<7>(T->lens + 296, 19, T->pre_count, T->pre_first, T->pre_offs, T->pre_sorted,
+                      T->next, T->pre_lut, lane, pre_entry);
+  if (!ok) return kBadDeflate;
+  int i = 0, total = nlen + ndist;
+  uint32_t prev = 0;
+  while (i < total) {
+    br.refill(lane);
+    if (br.overrun()) {
+      ok = false;
+      break;
+    }
+    uint32_t e = T->pre_lut[br.bb & 127];
+    uint32_t L = e & 15;
+    if (L == 0) {
+      ok = false;
+      break;
+    }
+    uint32_t sym = e >> 16;
+    br.consume(L);
+    if (sym < 16) {
+      if (lane == 0) T->lens[i] = (uint8_t)sym;
+      prev = sym;
+      i++;
+      continue;
+    }
+    int rep;
+    uint32_t v = 0;
+    if (sym == 16) {
+      if (i == 0) {
+        ok = false;
+        break;
+      }
+      v = prev;
+      rep = 3 + (int)(br.bb & 3);
+      br.consume(2);
+    } else if (sym == 17) {
+      rep = 3 + (int)(br.bb & 7);
+      br.consume(3);
+    } else {
+      rep = 11 + (int)(br.bb & 127);
+      br.consume(7);
+    }
+    if (i + rep > total) {
+      ok = false;
+      break;
+    }
+    for (int j = lane; j < rep; j += 32) T->lens[i + j] = (uint8_t)v;
+    prev = v;
+    i += rep;
+  }
+  __syncwarp();
+  if (br.overrun()) return br.wpos > trunc_words ? kTruncated : kOvershoot;
+  if (!ok || T->lens[256] == 0) return kBadDeflate;
+  // the dist lengths must not alias the precode area: move them to 288+
+  uint8_t dl = lane < ndist ? T->lens[nlen + lane] : 0;
+  __syncwarp();
+  T->lens[288 + lane] = lane < ndist ? dl : 0;
+  __syncwarp();
+  ok = build_table<LB>(T->lens, nlen, T->lit_count, T->lit_first, T->lit_offs, T->lit_sorted,
+                       T->next, T->lit_lut, lane, litlen_entry);
+  ok = ok && build_table<kDistBits>(T->lens + 288, ndist, T->dist_count, T->dist_first,
+                                    T->dist_offs, T->dist_sorted, T->next, T->dist_lut, lane,
+                                    dist_entry);
+  return ok ? kOk : kBadDeflate;
+}
+
 // ---------------------------------------------------------------------------
-// Output pages
+// Page allocation (both layouts).
 // ---------------------------------------------------------------------------
-struct PageWriter {
-  uint32_t page;       // current page (kNoPage before the first)
-  uint32_t prev;       // previous page
-  uint32_t fill;       // entries in the current page
+__device__ __forceinline__ uint32_t alloc_page(const PagePool& pool, uint32_t cid, uint32_t gen,
+                                               uint32_t seq, int lane) {
+  uint32_t p = 0;
+  if (lane == 0) {
+    p = atomicAdd(pool.next, 1u);
+    if (p < pool.cap) {
+      pool.owner[p] = cid;
+      pool.seq[p] = (gen << kGenShift) | seq;
+    }
+  }
+  p = __shfl_sync(0xFFFFFFFFu, p, 0);
+  return p < pool.cap ? p : kNoPage;
+}
+
+// ---------------------------------------------------------------------------
+// History in the chunk's own pages.
+//   seq s = index of the page holding the current output position o; the
+//   pages of seq s-1, s, s+1 are kept in registers.  A back-reference reads
+//   [o - 32768, o): seq s-1 or s.  A symbol writes [o, o + 258): seq s or s+1.
+// ---------------------------------------------------------------------------
+struct PageHist {
+  uint16_t* data;
+  uint32_t prev, cur, next;  // page ids of seq s-1, s, s+1 (kNoPage = none)
+  uint64_t s;
   uint32_t n_pages;
   bool failed;
 
-  __device__ __forceinline__ bool ensure(const PagePool& pool, uint32_t cid, int lane) {
+  __device__ __forceinline__ uint16_t* at(uint64_t q) const {
+    uint64_t qs = q >> 16;
+    uint32_t pg = qs == s ? cur : (qs < s ? prev : next);
+    return data + (size_t)pg * kPageEntries + (q & (kPageEntries - 1));
+  }
+  __device__ __forceinline__ uint32_t page_of_seq(uint64_t x) const {
+    return x == s ? cur : (x + 1 == s ? prev : (x == s + 1 ? next : kNoPage));
+  }
+  // make positions [o, o_end) writable (o_end - o <= kPageEntries)
+  __device__ __forceinline__ bool ensure(const PagePool& pool, uint32_t cid, uint32_t gen,
+                                         uint64_t o_end, int lane) {
+    if (cur == kNoPage) {
+      cur = alloc_page(pool, cid, gen, (uint32_t)s, lane);
+      n_pages++;
+      if (cur == kNoPage) return failed = true, false;
+    }
+    if (((o_end - 1) >> 16) > s && next == kNoPage) {
+      next = alloc_page(pool, cid, gen, (uint32_t)(s + 1), lane);
+      n_pages++;
+      if (next == kNoPage) return failed = true, false;
+    }
+    return true;
+  }
+  __device__ __forceinline__ void advance(uint64_t o) {
+    if ((o >> 16) > s) {
+      prev = cur;
+      cur = next;
+      next = kNoPage;
+      s++;
+    }
+  }
+};
+
+// ---------------------------------------------------------------------------
+// Ring history in shared memory, flushed to pages.
+// ---------------------------------------------------------------------------
+struct PageWriter {
+  uint32_t page;  // current page (kNoPage before the first)
+  uint32_t prev;  // previous page
+  uint32_t fill;  // entries in the current page
+  uint32_t n_pages;
+  bool failed;
+
+  __device__ __forceinline__ bool ensure(const PagePool& pool, uint32_t cid, uint32_t gen,
+                                         int lane) {
     if (page != kNoPage && fill < kPageEntries) return true;
-    uint32_t p = 0;
-    if (lane == 0) {
-      p = atomicAdd(pool.next, 1u);
-      if (p < pool.cap) {
-        pool.owner[p] = cid;
-        pool.seq[p] = n_pages;
-      }
-    }
-    p = __shfl_sync(0xFFFFFFFFu, p, 0);
-    if (p >= pool.cap) {
-      failed = true;
-      return false;
-    }
+    uint32_t p = alloc_page(pool, cid, gen, n_pages, lane);
+    if (p == kNoPage) return failed = true, false;
     prev = page;
     page = p;
     fill = 0;
@@ -250,12 +428,12 @@ struct PageWriter {
   }
 };
 
-template <int LB>
-__device__ __forceinline__ bool flush_full(WarpSmem<LB>* S, PageWriter& pw, const PagePool& pool,
-                                           uint64_t& flushed, uint32_t cid, int lane) {
-  if (!pw.ensure(pool, cid, lane)) return false;
+__device__ __forceinline__ bool ring_flush_full(uint16_t* ring, PageWriter& pw,
+                                                const PagePool& pool, uint64_t& flushed,
+                                                uint32_t cid, uint32_t gen, int lane) {
+  if (!pw.ensure(pool, cid, gen, lane)) return false;
   __syncwarp();
-  const uint4* src = reinterpret_cast<const uint4*>(S->ring + ((uint32_t)flushed & kRingMask));
+  const uint4* src = reinterpret_cast<const uint4*>(ring + ((uint32_t)flushed & kRingMask));
   uint4* dst = reinterpret_cast<uint4*>(pool.data + (size_t)pw.page * kPageEntries + pw.fill);
 #pragma unroll 4
   for (int k = lane; k < (int)(kFlush / 8); k += 32) dst[k] = src[k];
@@ -264,17 +442,17 @@ __device__ __forceinline__ bool flush_full(WarpSmem<LB>* S, PageWriter& pw, cons
   return true;
 }
 
-template <int LB>
-__device__ bool flush_tail(WarpSmem<LB>* S, PageWriter& pw, const PagePool& pool,
-                           uint64_t& flushed, uint64_t o, uint32_t cid, int lane) {
+__device__ bool ring_flush_tail(const uint16_t* ring, PageWriter& pw, const PagePool& pool,
+                                uint64_t& flushed, uint64_t o, uint32_t cid, uint32_t gen,
+                                int lane) {
   __syncwarp();
   while (flushed < o) {
-    if (!pw.ensure(pool, cid, lane)) return false;
+    if (!pw.ensure(pool, cid, gen, lane)) return false;
     uint32_t r = (uint32_t)(o - flushed);
     uint32_t room = kPageEntries - pw.fill;
     uint32_t k = r < room ? r : room;
     uint16_t* dst = pool.data + (size_t)pw.page * kPageEntries + pw.fill;
-    for (uint32_t j = lane; j < k; j += 32) dst[j] = S->ring[((uint32_t)flushed + j) & kRingMask];
+    for (uint32_t j = lane; j < k; j += 32) dst[j] = ring[((uint32_t)flushed + j) & kRingMask];
     pw.fill += k;
     flushed += k;
   }
@@ -282,44 +460,56 @@ __device__ bool flush_tail(WarpSmem<LB>* S, PageWriter& pw, const PagePool& pool
 }
 
 // ---------------------------------------------------------------------------
-// Decode one chunk.
+// Decode one chunk.  kRing selects the history layout.
 // ---------------------------------------------------------------------------
-template <int LB>
-__device__ void decode_chunk(const uint8_t* __restrict__ in, const ChunkDesc& d, ChunkResult* res,
-                             uint32_t cid, WarpSmem<LB>* S, const PagePool& pool, int lane) {
+template <int LB, bool kRing>
+__device__ int32_t decode_chunk(const uint8_t* __restrict__ in, const ChunkDesc& d,
+                                ChunkResult* res, uint32_t cid, uint32_t gen, uint16_t* ring,
+                                Tables<LB>* T, const PagePool& pool, int lane) {
   const bool zero_window = (d.flags & kChunkMemberFirst) != 0;
-  // seed the ring: zeros for a member start, marker values otherwise
-  for (uint32_t i = lane * 8; i < kWindow; i += 256) {
-    uint4 v;
-    if (zero_window) {
-      v = make_uint4(0, 0, 0, 0);
-    } else {
-      uint32_t b = kMarkerBase + i;
-      v.x = b | ((b + 1) << 16);
-      v.y = (b + 2) | ((b + 3) << 16);
-      v.z = (b + 4) | ((b + 5) << 16);
-      v.w = (b + 6) | ((b + 7) << 16);
+  if (kRing) {
+    // seed the ring: zeros for a member start, marker values otherwise
+    for (uint32_t i = lane * 8; i < kWindow; i += 256) {
+      uint4 v;
+      if (zero_window) {
+        v = make_uint4(0, 0, 0, 0);
+      } else {
+        uint32_t b = kMarkerBase + i;
+        v.x = b | ((b + 1) << 16);
+        v.y = (b + 2) | ((b + 3) << 16);
+        v.z = (b + 4) | ((b + 5) << 16);
+        v.w = (b + 6) | ((b + 7) << 16);
+      }
+      *reinterpret_cast<uint4*>(ring + i) = v;
     }
-    *reinterpret_cast<uint4*>(S->ring + i) = v;
+    __syncwarp();
   }
-  __syncwarp();
 
   BitReader br;
   br.in32 = reinterpret_cast<const uint32_t*>(in);
-  br.limit_words = (d.in_end * 8 + 31) / 32 + 2;
+  const uint64_t trunc_words = (d.in_end * 8 + 31) / 32 + 2;
+  br.limit_words = trunc_words;
+  if (d.abort_bit != kNoStop && d.abort_bit / 32 + 2 < trunc_words) br.limit_words = d.abort_bit / 32 + 2;
   br.seek(d.start_bit, lane);
   br.refill(lane);
 
+  PageHist ph{pool.data, kNoPage, kNoPage, kNoPage, 0, 0, false};
   PageWriter pw{kNoPage, kNoPage, 0, 0, false};
   uint64_t o = 0, flushed = 0, marker_end = 0;
   uint32_t n_blocks = 0;
   int32_t status = kOk, final_block = 0;
   const uint64_t in_end_bits = d.in_end * 8;
   constexpr uint32_t LMASK = (1u << LB) - 1, DMASK = (1u << kDistBits) - 1;
+  // page-history fast path: positions below `guard` need no page work
+  uint64_t guard = 0;
 
   for (;;) {
     uint64_t bitpos = br.pos();
     if (bitpos >= d.stop_lo) break;
+    if (bitpos > d.abort_bit) {
+      status = kOvershoot;
+      break;
+    }
     if (bitpos + 3 > in_end_bits) {
       status = kTruncated;
       break;
@@ -349,151 +539,55 @@ __device__ void decode_chunk(const uint8_t* __restrict__ in, const ChunkDesc& d,
       }
       uint32_t done = 0;
       while (done < ln) {
-        if (o - flushed >= kFlush) {
-          if (!flush_full(S, pw, pool, flushed, cid, lane)) break;
-        }
         uint32_t k = ln - done;
         if (k > 4096) k = 4096;
         const uint8_t* src = in + byte + done;
-        for (uint32_t j = lane; j < k; j += 32) S->ring[(uint32_t)(o + j) & kRingMask] = src[j];
+        if (kRing) {
+          if (o - flushed >= kFlush && !ring_flush_full(ring, pw, pool, flushed, cid, gen, lane)) break;
+          for (uint32_t j = lane; j < k; j += 32) ring[(uint32_t)(o + j) & kRingMask] = src[j];
+        } else {
+          ph.advance(o);
+          if (!ph.ensure(pool, cid, gen, o + k, lane)) break;
+          for (uint32_t j = lane; j < k; j += 32) *ph.at(o + j) = src[j];
+        }
         o += k;
         done += k;
         __syncwarp();
       }
-      if (pw.failed) {
+      if (pw.failed || ph.failed) {
         status = kPoolExhausted;
         break;
       }
+      guard = 0;
       br.seek((byte + ln) * 8, lane);
     } else if (btype == 1 || btype == 2) {
-      bool ok;
-      if (btype == 1) {
-        // fixed Huffman (RFC 1951 3.2.6)
-        for (int s = lane; s < 320; s += 32) {
-          uint8_t l;
-          if (s < 144) l = 8;
-          else if (s < 256) l = 9;
-          else if (s < 280) l = 7;
-          else if (s < 288) l = 8;
-          else l = 5;  // 288..319: 32 distance codes of 5 bits
-          S->lens[s] = l;
-        }
-        __syncwarp();
-        ok = build_table<LB>(S->lens, 288, S->lit_count, S->lit_first, S->lit_offs, S->lit_sorted,
-                             S->next, S->lit_lut, lane, litlen_entry);
-        ok = ok && build_table<kDistBits>(S->lens + 288, 32, S->dist_count, S->dist_first,
-                                          S->dist_offs, S->dist_sorted, S->next, S->dist_lut,
-                                          lane, dist_entry);
-      } else {
-        // dynamic header (RFC 1951 3.2.7)
-        br.refill(lane);
-        uint32_t h = (uint32_t)br.bb & 0x3FFF;
-        br.consume(14);
-        int nlen = 257 + (h & 31), ndist = 1 + ((h >> 5) & 31), ncl = 4 + (h >> 10);
-        if (nlen > 286 || ndist > 30) {
-          status = kBadDeflate;
-          break;
-        }
-        // code-length code lengths: 3 bits each, read as up to 10 + 9
-        uint32_t clv = 0;
-        int n1 = ncl < 10 ? ncl : 10;
-        br.refill(lane);
-        if (lane < n1) clv = (uint32_t)(br.bb >> (3 * lane)) & 7;
-        br.consume(3 * n1);
-        br.refill(lane);
-        if (lane >= 10 && lane < ncl) clv = (uint32_t)(br.bb >> (3 * (lane - 10))) & 7;
-        br.consume(3 * (ncl - n1));
-        if (lane < 19) S->lens[296 + c_cl_order[lane]] = (uint8_t)clv;
-        __syncwarp();
-        ok = build_table<7>(S->lens + 296, 19, S->pre_count, S->pre_first, S->pre_offs,
-                            S->pre_sorted, S->next, S->pre_lut, lane, pre_entry);
-        if (!ok) {
-          status = kBadDeflate;
-          break;
-        }
-        int i = 0, total = nlen + ndist;
-        uint32_t prev = 0;
-        while (i < total) {
-          br.refill(lane);
-          if (br.overrun()) {
-            ok = false;
-            break;
-          }
-          uint32_t e = S->pre_lut[br.bb & 127];
-          uint32_t L = e & 15;
-          if (L == 0) {
-            ok = false;
-            break;
-          }
-          uint32_t sym = e >> 16;
-          br.consume(L);
-          if (sym < 16) {
-            if (lane == 0) S->lens[i] = (uint8_t)sym;
-            prev = sym;
-            i++;
-            continue;
-          }
-          int rep;
-          uint32_t v = 0;
-          if (sym == 16) {
-            if (i == 0) {
-              ok = false;
-              break;
-            }
-            v = prev;
-            rep = 3 + (int)(br.bb & 3);
-            br.consume(2);
-          } else if (sym == 17) {
-            rep = 3 + (int)(br.bb & 7);
-            br.consume(3);
-          } else {
-            rep = 11 + (int)(br.bb & 127);
-            br.consume(7);
-          }
-          if (i + rep > total) {
-            ok = false;
-            break;
-          }
-          for (int j = lane; j < rep; j += 32) S->lens[i + j] = (uint8_t)v;
-          prev = v;
-          i += rep;
-        }
-        __syncwarp();
-        if (!ok || S->lens[256] == 0 || br.overrun()) {
-          status = br.overrun() ? kTruncated : kBadDeflate;
-          break;
-        }
-        // the dist lengths must not alias the precode area: move them to 288+
-        uint8_t dl = lane < ndist ? S->lens[nlen + lane] : 0;
-        __syncwarp();
-        if (lane < 32) S->lens[288 + lane] = lane < ndist ? dl : 0;
-        __syncwarp();
-        ok = build_table<LB>(S->lens, nlen, S->lit_count, S->lit_first, S->lit_offs, S->lit_sorted,
-                             S->next, S->lit_lut, lane, litlen_entry);
-        ok = ok && build_table<kDistBits>(S->lens + 288, ndist, S->dist_count, S->dist_first,
-                                          S->dist_offs, S->dist_sorted, S->next, S->dist_lut,
-                                          lane, dist_entry);
-      }
-      if (!ok) {
-        status = kBadDeflate;
-        break;
-      }
+      status = read_tables<LB>(br, btype, T, trunc_words, lane);
+      if (status != kOk) break;
       // Huffman-coded block body
       for (;;) {
-        if (o - flushed >= kFlush) {
-          if (!flush_full(S, pw, pool, flushed, cid, lane)) {
+        if (kRing) {
+          if (o - flushed >= kFlush && !ring_flush_full(ring, pw, pool, flushed, cid, gen, lane)) {
             status = kPoolExhausted;
             break;
           }
+        } else if (o >= guard) {
+          ph.advance(o);
+          if (!ph.ensure(pool, cid, gen, o + 258, lane)) {
+            status = kPoolExhausted;
+            break;
+          }
+          // o + 258 stays inside the mapped pages until o reaches guard
+          uint64_t pe = (ph.s + 1) << 16;  // end of the current page
+          guard = ph.next != kNoPage ? pe : pe - 258;
         }
         br.refill(lane);
         if (br.overrun()) {
-          status = kTruncated;
+          status = br.wpos > trunc_words ? kTruncated : kOvershoot;
           break;
         }
-        uint32_t e = S->lit_lut[br.bb & LMASK];
+        uint32_t e = T->lit_lut[br.bb & LMASK];
         if ((e & 15) == 0) {
-          e = slow_decode<LB>(br.bb, S->lit_count, S->lit_first, S->lit_offs, S->lit_sorted,
+          e = slow_decode<LB>(br.bb, T->lit_count, T->lit_first, T->lit_offs, T->lit_sorted,
                               litlen_entry);
           if (e == 0) {
             status = kBadDeflate;
@@ -503,7 +597,10 @@ __device__ void decode_chunk(const uint8_t* __restrict__ in, const ChunkDesc& d,
         uint32_t L = e & 15, kind = (e >> 8) & 3;
         if (kind == kKindLit) {
           br.consume(L);
-          if (lane == 0) S->ring[(uint32_t)o & kRingMask] = (uint16_t)(e >> 16);
+          if (lane == 0) {
+            if (kRing) ring[(uint32_t)o & kRingMask] = (uint16_t)(e >> 16);
+            else *ph.at(o) = (uint16_t)(e >> 16);
+          }
           o++;
           continue;
         }
@@ -519,10 +616,10 @@ __device__ void decode_chunk(const uint8_t* __restrict__ in, const ChunkDesc& d,
         uint32_t len = (e >> 16) + (uint32_t)((br.bb >> L) & ((1u << xb) - 1));
         br.consume(L + xb);
         br.refill(lane);
-        uint32_t de = S->dist_lut[br.bb & DMASK];
+        uint32_t de = T->dist_lut[br.bb & DMASK];
         if ((de & 15) == 0) {
-          de = slow_decode<kDistBits>(br.bb, S->dist_count, S->dist_first, S->dist_offs,
-                                      S->dist_sorted, dist_entry);
+          de = slow_decode<kDistBits>(br.bb, T->dist_count, T->dist_first, T->dist_offs,
+                                      T->dist_sorted, dist_entry);
           if (de == 0) {
             status = kBadDeflate;
             break;
@@ -542,20 +639,32 @@ __device__ void decode_chunk(const uint8_t* __restrict__ in, const ChunkDesc& d,
         // LZ77 copy: entry o+j = entry o-dist+(j mod dist); every source is
         // older than o, so the 32-wide steps are independent.
         __syncwarp();
-        const uint32_t ob = (uint32_t)o;
         const bool wrap = dist < len;
+        const uint32_t step_mod = wrap ? 32 % dist : 0;
+        uint32_t r = wrap ? (uint32_t)lane % dist : (uint32_t)lane;  // j mod dist for j = lane
         for (uint32_t j0 = 0; j0 < len; j0 += 32) {
           const uint32_t j = j0 + lane;
           const bool act = j < len;
           uint16_t v = 0;
           if (act) {
-            uint32_t sj = wrap ? j % dist : j;
-            v = S->ring[(ob - dist + sj) & kRingMask];
-            S->ring[(ob + j) & kRingMask] = v;
+            const uint32_t sj = wrap ? r : j;
+            if (kRing) {
+              v = ring[((uint32_t)o - dist + sj) & kRingMask];
+              ring[((uint32_t)o + j) & kRingMask] = v;
+            } else {
+              const int64_t sp = (int64_t)o - (int64_t)dist + (int64_t)sj;
+              if (sp >= 0) v = *ph.at((uint64_t)sp);
+              else v = zero_window ? 0 : (uint16_t)(kMarkerBase + kWindow + sp);
+              *ph.at(o + j) = v;
+            }
           }
           if (!zero_window) {
             uint32_t m = __ballot_sync(0xFFFFFFFFu, act && v >= kMarkerBase);
             if (m) marker_end = o + j0 + 32 - __clz(m);
+          }
+          if (wrap) {
+            r += step_mod;
+            if (r >= dist) r -= dist;
           }
         }
         o += len;
@@ -574,30 +683,46 @@ __device__ void decode_chunk(const uint8_t* __restrict__ in, const ChunkDesc& d,
   }
   uint64_t end_bit = br.pos();
   if (status == kOk && end_bit > in_end_bits) status = kTruncated;
-  if (status == kOk && !flush_tail(S, pw, pool, flushed, o, cid, lane)) status = kPoolExhausted;
+  uint32_t last_page = kNoPage, prev_page = kNoPage, n_pages = 0;
+  if (kRing) {
+    if (status == kOk && !ring_flush_tail(ring, pw, pool, flushed, o, cid, gen, lane)) status = kPoolExhausted;
+    last_page = pw.page;
+    prev_page = pw.prev;
+    n_pages = pw.n_pages;
+  } else {
+    __syncwarp();
+    if (o > 0) {
+      ph.advance(o - 1);
+      uint64_t ls = (o - 1) >> 16;
+      last_page = ph.page_of_seq(ls);
+      prev_page = ls > 0 ? ph.page_of_seq(ls - 1) : kNoPage;
+    }
+    n_pages = ph.n_pages;
+  }
   if (lane == 0) {
     res->end_bit = end_bit;
     res->out_len = o;
     res->marker_end = marker_end;
-    res->last_page = pw.page;
-    res->prev_page = pw.prev;
-    res->n_pages = pw.n_pages;
+    res->last_page = last_page;
+    res->prev_page = prev_page;
+    res->n_pages = n_pages;
     res->n_blocks = n_blocks;
     res->status = status;
     res->final_block = final_block;
+    res->gen = gen;
   }
   __syncwarp();
+  return status;
 }
 
-template <int LB>
-__global__ void __launch_bounds__(32 * kDecodeWarps)
-    inflate_kernel(const uint8_t* __restrict__ in, const ChunkDesc* __restrict__ descs,
-                   ChunkResult* __restrict__ results, const uint32_t* __restrict__ work,
-                   const uint32_t* __restrict__ n_work_ptr, uint32_t* work_counter, PagePool pool) {
-  const uint32_t n_work = *n_work_ptr;
-  extern __shared__ __align__(16) uint8_t smem[];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  WarpSmem<LB>* S = reinterpret_cast<WarpSmem<LB>*>(smem + warp * sizeof(WarpSmem<LB>));
+// Work loop shared by both kernels: take chunks from the queue; a failed
+// speculative start moves on to the next candidate of its partition.
+template <int LB, bool kRing>
+__device__ __forceinline__ void work_loop(const uint8_t* __restrict__ in, ChunkDesc* descs,
+                                          ChunkResult* results, const uint32_t* work,
+                                          uint32_t n_work, uint32_t* work_counter,
+                                          const PagePool& pool, uint16_t* ring, Tables<LB>* T,
+                                          int lane) {
   for (;;) {
     uint32_t w = 0;
     if (lane == 0) w = atomicAdd(work_counter, 1u);
@@ -605,43 +730,105 @@ __global__ void __launch_bounds__(32 * kDecodeWarps)
     if (w >= n_work) break;
     uint32_t cid = work[w];
     ChunkDesc d = descs[cid];
-    decode_chunk<LB>(in, d, &results[cid], cid, S, pool, lane);
+    uint64_t t0 = 0;
+    if (lane == 0) asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
+    const bool speculative = !(d.flags & kChunkMemberFirst) && d.limit_bit > d.lo_bit;
+    for (uint32_t gen = 0;; gen++) {
+      int32_t st = decode_chunk<LB, kRing>(in, d, &results[cid], cid, gen, ring, T, pool, lane);
+      if (st == kOk || st == kPoolExhausted || !speculative || gen + 1 >= kMaxTries) break;
+      uint64_t lo = 0, hi = 0;
+      if (!warp_find_first(in, d.in_end, d.lo_bit + 1, d.limit_bit, lane, lo, hi)) break;
+      d.lo_bit = lo;
+      d.start_bit = hi;
+      if (lane == 0) {
+        descs[cid].lo_bit = lo;
+        descs[cid].start_bit = hi;
+      }
+      __syncwarp();
+    }
+    if (lane == 0) {
+      uint64_t t1;
+      asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t1));
+      results[cid].t_start = t0;
+      results[cid].t_end = t1;
+    }
   }
 }
 
 template <int LB>
-size_t inflate_smem_bytes() {
-  return sizeof(WarpSmem<LB>) * kDecodeWarps;
+__global__ void __launch_bounds__(32 * kRingWarps)
+    inflate_ring_kernel(const uint8_t* __restrict__ in, ChunkDesc* __restrict__ descs,
+                        ChunkResult* __restrict__ results, const uint32_t* __restrict__ work,
+                        const uint32_t* __restrict__ n_work_ptr, uint32_t* work_counter,
+                        PagePool pool) {
+  extern __shared__ __align__(16) uint8_t smem[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  RingSmem<LB>* S = reinterpret_cast<RingSmem<LB>*>(smem) + warp;
+  work_loop<LB, true>(in, descs, results, work, *n_work_ptr, work_counter, pool, S->ring, &S->t,
+                      lane);
 }
 
 template <int LB>
-cudaError_t launch_inflate(const uint8_t* in, const ChunkDesc* descs, ChunkResult* results,
+__global__ void __launch_bounds__(32 * kPageWarps, kPageMinBlocks)
+    inflate_pages_kernel(const uint8_t* __restrict__ in, ChunkDesc* __restrict__ descs,
+                         ChunkResult* __restrict__ results, const uint32_t* __restrict__ work,
+                         const uint32_t* __restrict__ n_work_ptr, uint32_t* work_counter,
+                         PagePool pool) {
+  extern __shared__ __align__(16) uint8_t smem[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  Tables<LB>* T = reinterpret_cast<Tables<LB>*>(smem) + warp;
+  work_loop<LB, false>(in, descs, results, work, *n_work_ptr, work_counter, pool, nullptr, T,
+                       lane);
+}
+
+template <int LB>
+size_t inflate_smem_bytes(bool ring) {
+  return ring ? sizeof(RingSmem<LB>) * kRingWarps : sizeof(Tables<LB>) * kPageWarps;
+}
+
+template <int LB>
+cudaError_t launch_inflate(bool ring, const uint8_t* in, ChunkDesc* descs, ChunkResult* results,
                            const uint32_t* work, const uint32_t* n_work, uint32_t* work_counter,
                            const PagePool& pool, int blocks, cudaStream_t stream) {
-  size_t smem = inflate_smem_bytes<LB>();
-  cudaError_t e = cudaFuncSetAttribute(inflate_kernel<LB>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return e;
-  inflate_kernel<LB><<<blocks, 32 * kDecodeWarps, smem, stream>>>(in, descs, results, work,
-                                                                   n_work, work_counter, pool);
+  size_t smem = inflate_smem_bytes<LB>(ring);
+  cudaError_t e;
+  if (ring) {
+    e = cudaFuncSetAttribute(inflate_ring_kernel<LB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem);
+    if (e != cudaSuccess) return e;
+    inflate_ring_kernel<LB><<<blocks, 32 * kRingWarps, smem, stream>>>(in, descs, results, work,
+                                                                       n_work, work_counter, pool);
+  } else {
+    e = cudaFuncSetAttribute(inflate_pages_kernel<LB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem);
+    if (e != cudaSuccess) return e;
+    inflate_pages_kernel<LB><<<blocks, 32 * kPageWarps, smem, stream>>>(in, descs, results, work,
+                                                                        n_work, work_counter, pool);
+  }
   return cudaGetLastError();
 }
 
 template <int LB>
-int inflate_blocks_per_sm() {
+int inflate_blocks_per_sm(bool ring) {
   int n = 0;
-  cudaFuncSetAttribute(inflate_kernel<LB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)inflate_smem_bytes<LB>());
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, inflate_kernel<LB>, 32 * kDecodeWarps,
-                                                inflate_smem_bytes<LB>());
+  size_t smem = inflate_smem_bytes<LB>(ring);
+  if (ring) {
+    cudaFuncSetAttribute(inflate_ring_kernel<LB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, inflate_ring_kernel<LB>, 32 * kRingWarps, smem);
+  } else {
+    cudaFuncSetAttribute(inflate_pages_kernel<LB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, inflate_pages_kernel<LB>, 32 * kPageWarps, smem);
+  }
   return n;
 }
 
-#define GZGPU_INST(LB)                                                                      \
-  template size_t inflate_smem_bytes<LB>();                                                 \
-  template int inflate_blocks_per_sm<LB>();                                                 \
-  template cudaError_t launch_inflate<LB>(const uint8_t*, const ChunkDesc*, ChunkResult*,   \
-                                          const uint32_t*, const uint32_t*, uint32_t*,      \
+#define GZGPU_INST(LB)                                                                        \
+  template size_t inflate_smem_bytes<LB>(bool);                                               \
+  template int inflate_blocks_per_sm<LB>(bool);                                               \
+  template cudaError_t launch_inflate<LB>(bool, const uint8_t*, ChunkDesc*, ChunkResult*,     \
+                                          const uint32_t*, const uint32_t*, uint32_t*,        \
                                           const PagePool&, int, cudaStream_t);
 GZGPU_INST(10)
 GZGPU_INST(11)

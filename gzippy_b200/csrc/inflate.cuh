@@ -1,4 +1,4 @@
-// inflate.cuh -- launch interface of the chunk inflate kernel.
+// inflate.cuh -- launch interface of the chunk inflate kernels.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -6,15 +6,17 @@
 
 namespace gzgpu {
 
-constexpr int kDecodeWarps = 1;  // warps (= chunks in flight) per CTA
-constexpr int kDistBits = 8;     // distance LUT index bits
+constexpr int kRingWarps = 1;      // ring kernel: warps per CTA (64 KB ring each)
+constexpr int kPageWarps = 8;      // page kernel: warps per CTA (tables only)
+constexpr int kPageMinBlocks = 4;  // page kernel: CTAs per SM the registers are sized for
+constexpr int kDistBits = 8;       // distance LUT index bits
 
 template <int LB>
-size_t inflate_smem_bytes();
+size_t inflate_smem_bytes(bool ring);
 template <int LB>
-int inflate_blocks_per_sm();
+int inflate_blocks_per_sm(bool ring);
 template <int LB>
-cudaError_t launch_inflate(const uint8_t* in, const ChunkDesc* descs, ChunkResult* results,
+cudaError_t launch_inflate(bool ring, const uint8_t* in, ChunkDesc* descs, ChunkResult* results,
                            const uint32_t* work, const uint32_t* n_work, uint32_t* work_counter,
                            const PagePool& pool, int blocks, cudaStream_t stream);
 

@@ -6,8 +6,12 @@
 // member_scan_kernel: every byte position of every stream is tested like
 //   scan_member_boundaries_fast (src/decompress/bgzf.rs:2090-2230): bytes
 //   1f 8b 08, FLG & 0xE0 == 0, pos >= 4, the preceding ISIZE in (0, 1 GiB],
-//   pos past the first header and pos + 10 < stream length.  Each hit's
-//   header is parsed (parse_gzip_header :2047) for its deflate start.
+//   pos past the first header and pos + 10 < stream length; plus the header
+//   plausibility of is_likely_multi_member (src/decompress/format.rs:92-125:
+//   MTIME, XFL, OS), which removes nearly every false hit in compressed data.
+//   A real member that fails it is still found by the host chain walk.
+//   Each hit's header is parsed (parse_gzip_header :2047) for its deflate
+//   start.
 #include <cstdint>
 
 #include "common.cuh"
@@ -89,6 +93,12 @@ __global__ void member_scan_kernel(const uint8_t* __restrict__ in, const ScanUni
       if (q[0] != 0x1f || q[1] != 0x8b || q[2] != 8 || (q[3] & 0xE0)) continue;
       uint32_t isz = q[-4] | (q[-3] << 8) | ((uint32_t)q[-2] << 16) | ((uint32_t)q[-1] << 24);
       if (isz == 0 || isz > (1u << 30)) continue;
+      // header plausibility of is_likely_multi_member (format.rs:92-125):
+      // MTIME 0 or <= 4102444800, XFL in {0, 2, 4}, OS <= 13 or 255
+      uint32_t mtime = q[4] | (q[5] << 8) | ((uint32_t)q[6] << 16) | ((uint32_t)q[7] << 24);
+      if (mtime > 4102444800u) continue;
+      if (q[8] != 0 && q[8] != 2 && q[8] != 4) continue;
+      if (q[9] > 13 && q[9] != 255) continue;
       uint32_t k = atomicAdd(n_cands, 1u);
       if (k < cap) {
         MemberCand c;

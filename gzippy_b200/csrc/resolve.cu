@@ -24,10 +24,12 @@
 
 namespace gzgpu {
 
+// page of entry q of a chunk's last 32 KiB: the page of its last entry or
+// the one before (a page holds 64 Ki entries)
 __device__ __forceinline__ const uint16_t* chunk_entry_page(const ChunkResult& r, uint64_t q,
                                                             const PagePool& pool) {
-  uint64_t seq = q / kPageEntries;
-  uint32_t page = (seq + 1 == r.n_pages) ? r.last_page : r.prev_page;
+  uint64_t last_seq = (r.out_len - 1) / kPageEntries;
+  uint32_t page = (q / kPageEntries == last_seq) ? r.last_page : r.prev_page;
   return pool.data + (size_t)page * kPageEntries;
 }
 
@@ -79,10 +81,12 @@ __global__ void body_kernel(const PlacedChunk* __restrict__ placed,
     uint32_t cid = pool.owner[p];
     uint32_t k = placed_of_chunk[cid];
     if (k == 0xFFFFFFFFu) continue;
+    const uint32_t sw = pool.seq[p];
+    if ((sw >> kGenShift) != results[cid].gen) continue;  // page of a failed attempt
     const PlacedChunk pc = placed[k];
     const uint64_t len = results[cid].out_len;
     const uint64_t t0 = len > kWindow ? len - kWindow : 0;
-    const uint64_t q0 = (uint64_t)pool.seq[p] * kPageEntries;
+    const uint64_t q0 = (uint64_t)(sw & kSeqMask) * kPageEntries;
     if (q0 >= t0) continue;
     uint64_t qend = q0 + kPageEntries;
     if (qend > t0) qend = t0;

@@ -51,6 +51,8 @@ typedef struct {
   size_t chunk_bytes; /* compressed bytes per speculative chunk; 0 = tuned default */
   int lut_bits;       /* litlen LUT index bits: 10, 11 or 12; 0 = tuned default */
   int autotune;       /* 1 = choose chunk_bytes / lut_bits per job from the tuning table */
+  int ring_history;   /* 1 = decode history in a shared-memory ring (3 warps/SM) instead
+                         of the output pages in HBM (32 warps/SM, the default) */
 } gzgpu_config;
 
 typedef struct {
@@ -127,6 +129,14 @@ int gzgpu_debug_find(gzgpu_ctx *ctx, const uint8_t *in, size_t in_len, const uin
 int gzgpu_debug_decode(gzgpu_ctx *ctx, const uint8_t *in, size_t in_len, const uint64_t *start,
                        const uint64_t *stop, const int *member_first, size_t n, uint16_t *entries,
                        size_t cap_per, uint64_t *res);
+
+/* gzgpu_debug_last_chunks: the chunk table of the last job.  descs holds
+ * n records of 64 bytes (start_bit, lo_bit, stop_lo, guess_bit, limit_bit,
+ * in_end, abort_bit as u64; flags, stream as u32); results n records of 72
+ * bytes (end_bit, out_len, marker_end as u64; last_page, prev_page, n_pages,
+ * n_blocks as u32; status, final_block as i32; t_start, t_end as u64 device
+ * nanoseconds; gen as u32 + 4 pad bytes: 72 bytes).  *n = records available (copies min(cap, *n)). */
+int gzgpu_debug_last_chunks(gzgpu_ctx *ctx, void *descs, void *results, size_t cap, size_t *n);
 
 /* Statistics of the last call. */
 int gzgpu_get_stats(gzgpu_ctx *ctx, gzgpu_stats *out);

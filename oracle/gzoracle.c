@@ -400,6 +400,7 @@ int orc_inflate_chunk(const uint8_t *data, size_t n, uint64_t start_bit, uint64_
         if (e) { st = e; break; }
       }
       for (;;) {
+        if (br_over(&b)) { st = ORC_TRUNCATED; break; }
         int sym = htab_decode(lit, &b);
         if (sym < 0) { st = ORC_BAD_DEFLATE; break; }
         if (sym < 256) {
@@ -713,7 +714,15 @@ static int find_first(const uint8_t *data, size_t n, uint64_t from, uint64_t to,
 /* Member scan: restates src/decompress/bgzf.rs scan_member_boundaries_fast    */
 /* :2090-2230 and parse_gzip_header :2047.  Returns 0 for "not multi-member". */
 /* ------------------------------------------------------------------------ */
+static size_t scan_members(const uint8_t *d, size_t n, orc_member *out, size_t cap, int strict);
+
 size_t orc_scan_members(const uint8_t *d, size_t n, orc_member *out, size_t cap) {
+  return scan_members(d, n, out, cap, 0);
+}
+
+/* strict: also require the header plausibility of is_likely_multi_member
+ * (src/decompress/format.rs:92-125: MTIME, XFL, OS), as the device scan does */
+static size_t scan_members(const uint8_t *d, size_t n, orc_member *out, size_t cap, int strict) {
   if (n < 18 || d[0] != 0x1f || d[1] != 0x8b || d[2] != 8) return 0;
   size_t h0 = 10;
   if (orc_gzip_header(d, n, &h0) != ORC_OK) h0 = 10;
@@ -729,7 +738,11 @@ size_t orc_scan_members(const uint8_t *d, size_t n, orc_member *out, size_t cap)
     if ((d[pos + 3] & 0xE0) == 0 && pos >= 4) {
       uint32_t is = d[pos - 4] | (d[pos - 3] << 8) | ((uint32_t)d[pos - 2] << 16) |
                     ((uint32_t)d[pos - 1] << 24);
-      if (is > 0 && is <= (1u << 30)) {
+      uint32_t mt = d[pos + 4] | (d[pos + 5] << 8) | ((uint32_t)d[pos + 6] << 16) |
+                    ((uint32_t)d[pos + 7] << 24);
+      int plausible = mt <= 4102444800u && (d[pos + 8] == 0 || d[pos + 8] == 2 || d[pos + 8] == 4) &&
+                      (d[pos + 9] <= 13 || d[pos + 9] == 255);
+      if (is > 0 && is <= (1u << 30) && (!strict || plausible)) {
         if (ns == scap) starts = (uint64_t *)realloc(starts, (scap *= 2) * sizeof(uint64_t));
         starts[ns++] = pos;
       }
@@ -929,11 +942,21 @@ static void decode_one(const uint8_t *in, size_t n, ochunk_t *c, uint64_t start)
   c->cap = cap;
 }
 
+/* A failed speculative start moves on to the next candidate of the same
+ * partition, up to 4 starts (speculative_decode_find_boundary,
+ * chunk_fetcher.rs:2616-2740, tries the candidates in order). */
 static void do_decode(void *a, size_t i) {
   cctx_t *x = (cctx_t *)a;
   ochunk_t *c = &x->c[i];
   if (!c->valid) return;
-  decode_one(x->in, x->n, c, c->hi);
+  for (int tries = 0;; tries++) {
+    decode_one(x->in, x->n, c, c->hi);
+    if (c->r.status == ORC_OK || c->member_first || tries + 1 >= 4) break;
+    uint64_t lo, hi;
+    if (!find_first(x->in, x->n, c->lo + 1, x->limit[i], &lo, &hi)) break;
+    c->lo = lo;
+    c->hi = hi;
+  }
 }
 
 typedef struct {
@@ -974,11 +997,11 @@ int orc_decompress_chunked(const uint8_t *in, size_t n, size_t chunk_bytes, int 
   uint64_t cbits = (uint64_t)chunk_bytes * 8;
 
   /* member ranges: scan candidates, else one member spanning the input */
-  size_t nm = orc_scan_members(in, n, NULL, 0);
+  size_t nm = scan_members(in, n, NULL, 0, 1);
   orc_member *mem = NULL;
   if (nm >= 2) {
     mem = (orc_member *)malloc(nm * sizeof(orc_member));
-    orc_scan_members(in, n, mem, nm);
+    scan_members(in, n, mem, nm, 1);
   } else {
     size_t hl;
     int hs = orc_gzip_header(in, n, &hl);
@@ -1023,7 +1046,9 @@ int orc_decompress_chunked(const uint8_t *in, size_t n, size_t chunk_bytes, int 
     ch[i].stop = ~0ull;
     for (size_t j = i + 1; j < nc; j++)
       if (ch[j].valid) {
-        ch[i].stop = ch[j].member_first ? ~0ull : ch[j].lo;
+        /* a member candidate ends its predecessor at its header bit: a real
+         * one follows the BFINAL block, a false one lies inside the member */
+        ch[i].stop = ch[j].member_first ? mem[ch[j].member].start * 8 : ch[j].lo;
         break;
       }
   }
@@ -1090,11 +1115,13 @@ int orc_decompress_chunked(const uint8_t *in, size_t n, size_t chunk_bytes, int 
         status = ORC_BAD_DEFLATE; /* no progress */
         break;
       }
-      while (j < nc && (!ch[j].valid || (!ch[j].member_first && ch[j].lo <= e))) {
+#define FIRST_BIT(k) (ch[k].member_first ? mem[ch[k].member].start * 8 : ch[k].lo)
+      while (j < nc && (!ch[j].valid || FIRST_BIT(j) <= e)) {
         if (ch[j].valid) st->n_spec_rejected++;
         j++;
       }
-      uint64_t stop = (j < nc && !ch[j].member_first) ? ch[j].lo : ~0ull;
+      uint64_t stop = j < nc ? FIRST_BIT(j) : ~0ull;
+#undef FIRST_BIT
       ochunk_t *rep;
       NEW_REPAIR(rep, e, stop, 0);
       cur = rep;

@@ -57,8 +57,10 @@ def test_finder_matches_oracle(ctx):
             assert g == exp, (f, t, g, exp)
 
 
-def test_decode_chunks_match_oracle(ctx):
+@pytest.mark.parametrize("ring", [False, True], ids=["pages", "ring"])
+def test_decode_chunks_match_oracle(G, ring):
     """Window-absent chunks from finder starts: entries, markers, end bits."""
+    ctx = G.Context(chunk_bytes=32 << 10, ring_history=ring)
     parts = [W.content(t, 5 + t, 1 << 20) for t in range(4)]
     plain = np.concatenate(parts)
     c = W.gzip_member(plain, 6)
@@ -86,12 +88,13 @@ def test_decode_chunks_match_oracle(ctx):
         assert np.array_equal(ent[i, :r.out_len], e), i
 
 
-def test_single_member_chunked_pipeline(G):
+@pytest.mark.parametrize("ring", [False, True], ids=["pages", "ring"])
+def test_single_member_chunked_pipeline(G, ring):
     parts = [W.content(t % 4, 100 + t, 1 << 20) for t in range(12)]
     plain = np.concatenate(parts)
     c = W.gzip_member(plain, 6, threads=4)
     for cb in (16 << 10, 64 << 10, 1 << 20):
-        ctx = G.Context(chunk_bytes=cb)
+        ctx = G.Context(chunk_bytes=cb, ring_history=ring)
         got = ctx.decompress(c)
         s = ctx.stats()
         ctx.close()
