@@ -179,6 +179,7 @@ def main():
     ap.add_argument("--scale", type=float, default=1.0)
     ap.add_argument("--chunk-bytes", type=int, default=0)
     ap.add_argument("--lut-bits", type=int, default=0)
+    ap.add_argument("--ctas-per-sm", type=int, default=0)
     ap.add_argument("--e2e-steps", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
@@ -239,7 +240,8 @@ def main():
     import gzippy_b200 as G
     comp, meta = load_workload(args.workload, args.scale)
     config.update(plain_bytes=meta["plain_bytes"], comp_bytes=meta["comp_bytes"])
-    ctx = G.Context(device=local, chunk_bytes=args.chunk_bytes, lut_bits=args.lut_bits)
+    ctx = G.Context(device=local, chunk_bytes=args.chunk_bytes, lut_bits=args.lut_bits,
+                    ctas_per_sm=args.ctas_per_sm)
 
     # device-resident buffers (torch only allocates device memory here)
     pad = 1024
@@ -332,6 +334,7 @@ def main():
             "data": "synthetic (seeded generator + zlib level 6)", "config": config,
             "byte_exact": byte_exact, "e2e": e2e, "roofline": roof, "clocks": clocks,
             "gpu_launches": int(launches),
+            "step_decode_ms": [round(x, 2) for x in dec_ms],
             "stages_ms": {k: round(getattr(st_last, k), 3) for k in
                           ("ms_scan", "ms_find", "ms_decode", "ms_decode_kernel", "ms_walk",
                            "ms_resolve", "ms_crc", "ms_total")},

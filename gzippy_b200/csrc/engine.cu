@@ -105,7 +105,21 @@ struct Walker {
   std::vector<uint32_t> order;
   std::vector<MemberPlan> members;
   uint32_t member_order_begin = 0;
-  int32_t pending = -1;     // repair chunk id awaiting decode
+  int32_t pending = -1;     // repair chunk id awaiting decode (walk suspended)
+  // Optimistic repairs: a repair is assumed to end exactly at the next
+  // candidate's start and the walk goes on; `cp` restores the walk if the
+  // decoded repair says otherwise.
+  struct Checkpoint {
+    size_t order_size, members_size;
+    uint32_t j, member, member_order_begin;
+    uint64_t mpos;
+  };
+  struct Assumption {
+    uint32_t repair;
+    uint64_t lo, hi;  // the next chunk's acceptable start range
+    Checkpoint cp;
+  };
+  std::vector<Assumption> assumed;
 };
 
 const char* kErrStr[] = {"ok",
@@ -133,6 +147,7 @@ struct gzgpu_ctx {
   int lut_bits = 10;
   bool autotune = false;
   bool ring = false;  // history layout of the inflate kernel (false = pages)
+  int ctas_per_sm = 3;  // page kernel CTAs per SM (3 or 4)
   int decode_blocks = 0;
   cudaEvent_t ev[12];
   gzgpu_stats stats{};
@@ -165,15 +180,15 @@ struct gzgpu_ctx {
     stats.decode_passes++;
     switch (lut_bits) {
       case 11:
-        return launch_inflate<11>(ring, cur_in, descs.as<ChunkDesc>(), results.as<ChunkResult>(),
+        return launch_inflate<11>(ring, ctas_per_sm, cur_in, descs.as<ChunkDesc>(), results.as<ChunkResult>(),
                                   work.as<uint32_t>(), d_work_count, counters.as<uint32_t>() + 3,
                                   pool, decode_blocks, st);
       case 12:
-        return launch_inflate<12>(ring, cur_in, descs.as<ChunkDesc>(), results.as<ChunkResult>(),
+        return launch_inflate<12>(ring, ctas_per_sm, cur_in, descs.as<ChunkDesc>(), results.as<ChunkResult>(),
                                   work.as<uint32_t>(), d_work_count, counters.as<uint32_t>() + 3,
                                   pool, decode_blocks, st);
       default:
-        return launch_inflate<10>(ring, cur_in, descs.as<ChunkDesc>(), results.as<ChunkResult>(),
+        return launch_inflate<10>(ring, ctas_per_sm, cur_in, descs.as<ChunkDesc>(), results.as<ChunkResult>(),
                                   work.as<uint32_t>(), d_work_count, counters.as<uint32_t>() + 3,
                                   pool, decode_blocks, st);
     }
@@ -182,9 +197,9 @@ struct gzgpu_ctx {
   int setup_decode_grid() {
     int per_sm = 1;
     switch (lut_bits) {
-      case 11: per_sm = inflate_blocks_per_sm<11>(ring); break;
-      case 12: per_sm = inflate_blocks_per_sm<12>(ring); break;
-      default: per_sm = inflate_blocks_per_sm<10>(ring); break;
+      case 11: per_sm = inflate_blocks_per_sm<11>(ring, ctas_per_sm); break;
+      case 12: per_sm = inflate_blocks_per_sm<12>(ring, ctas_per_sm); break;
+      default: per_sm = inflate_blocks_per_sm<10>(ring, ctas_per_sm); break;
     }
     if (per_sm < 1) per_sm = 1;
     decode_blocks = per_sm * sms;
@@ -199,11 +214,12 @@ struct gzgpu_ctx {
 };
 
 static uint64_t pick_chunk_bytes(uint64_t in_len) {
-  // enough chunks to fill every decoder slot several times over, but large
-  // enough that block-finder and marker overhead stay small
-  uint64_t c = 128 << 10;
-  if (in_len < (64ull << 20)) c = 64 << 10;
-  if (in_len < (4ull << 20)) c = 32 << 10;
+  // about two chunks per decoding warp on large inputs; smaller chunks for
+  // small inputs so the warps still fill (measured on the 1 GiB mixed stream:
+  // 64 KiB beats 32 KiB and 128 KiB)
+  uint64_t c = 64 << 10;
+  if (in_len < (64ull << 20)) c = 32 << 10;
+  if (in_len < (4ull << 20)) c = 16 << 10;
   return c;
 }
 
@@ -510,9 +526,7 @@ int gzgpu_ctx::run(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R) 
           w.done = true;
           break;
         }
-        uint64_t mlen = 0;
-        for (uint32_t k = w.member_order_begin; k < w.order.size(); k++) mlen += hr[w.order[k]].out_len;
-        w.members.push_back(MemberPlan{w.member_order_begin, (uint32_t)w.order.size(), trailer, mlen});
+        w.members.push_back(MemberPlan{w.member_order_begin, (uint32_t)w.order.size(), trailer, 0});
         w.member++;
         w.mpos = trailer + 8 - base;
         w.cur = -1;
@@ -535,6 +549,19 @@ int gzgpu_ctx::run(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R) 
       }
       w.j = j;
       uint64_t stop = j < w.c1 ? first_bit(j) : kNoStop;
+      if (j < w.c1 && !is_mf(j) && hr[j].status == kOk) {
+        // optimistic: the repair ends at the next candidate's start
+        Walker::Checkpoint cp{w.order.size(), w.members.size(), j, w.member,
+                              w.member_order_begin, w.mpos};
+        new_chunk(w, e, stop, 0);
+        uint32_t rid = (uint32_t)w.pending;
+        w.pending = -1;
+        w.assumed.push_back(Walker::Assumption{rid, hd[j].lo_bit, hd[j].start_bit, cp});
+        w.order.push_back(rid);
+        w.cur = (int32_t)j;
+        w.j = j + 1;
+        continue;
+      }
       new_chunk(w, e, stop, 0);
       break;
     }
@@ -580,10 +607,30 @@ int gzgpu_ctx::run(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R) 
     ms_dec_kernel += t;
     for (uint32_t k = 0; k < nr; k++)
       if (hr[base_id + k].status == kPoolExhausted) return kPoolExhausted;
-    for (uint32_t k = 0; k < nr; k++) {
-      Walker& w = W[repair_owner[k]];
-      w.cur = w.pending;
-      w.pending = -1;
+    for (Walker& w : W) {
+      if (w.pending >= 0) {
+        w.cur = w.pending;
+        w.pending = -1;
+      }
+      for (size_t a = 0; a < w.assumed.size(); a++) {
+        const Walker::Assumption& as = w.assumed[a];
+        if (as.repair < base_id) continue;  // verified in an earlier pass
+        const ChunkResult& rr = hr[as.repair];
+        if (rr.status == kOk && !rr.final_block && rr.end_bit >= as.lo && rr.end_bit <= as.hi)
+          continue;
+        // the repair ended elsewhere: resume the walk from it
+        w.order.resize(as.cp.order_size);
+        w.members.resize(as.cp.members_size);
+        w.j = as.cp.j;
+        w.member = as.cp.member;
+        w.member_order_begin = as.cp.member_order_begin;
+        w.mpos = as.cp.mpos;
+        w.cur = (int32_t)as.repair;
+        w.done = false;
+        w.status = kOk;
+        w.assumed.resize(a);
+        break;
+      }
     }
     repairs.clear();
     repair_owner.clear();
@@ -603,13 +650,16 @@ int gzgpu_ctx::run(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R) 
   std::vector<std::pair<uint32_t, uint32_t>> mem_owner;  // (stream, member)
   uint64_t out_total = 0;
   const uint64_t kCrcBlock = 64 << 10;
+  uint64_t last_marker_end = 0;
   for (uint32_t s = 0; s < ns; s++) {
     Walker& w = W[s];
     if (R[s].status == kOk) R[s].status = w.status;
     if (R[s].status != kOk) continue;
     R[s].out_off = out_total;
     uint64_t so = 0;
-    for (const MemberPlan& mp : w.members) {
+    for (MemberPlan& mp : w.members) {
+      mp.out_len = 0;
+      for (uint32_t k = mp.order_begin; k < mp.order_end; k++) mp.out_len += hr[w.order[k]].out_len;
       uint64_t moff = out_total + so;
       for (uint32_t k = mp.order_begin; k < mp.order_end; k++) {
         uint32_t cid = w.order[k];
@@ -617,7 +667,16 @@ int gzgpu_ctx::run(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R) 
         placed.push_back(PlacedChunk{out_total + so, moff, cid, 0});
         const ChunkResult& r = hr[cid];
         uint64_t t0 = r.out_len > kWindow ? r.out_len - kWindow : 0;
-        if (r.marker_end > t0) tlist.push_back((uint32_t)placed.size() - 1);
+        if (r.marker_end > t0) {
+          // a tail's markers read the 32 KiB before the chunk; they depend on
+          // the previous marker tail only if its output reaches into that
+          // window, otherwise a new independent run starts here
+          const uint64_t off = out_total + so;
+          if (tlist.size() > tseg.back() && last_marker_end + kWindow <= off)
+            tseg.push_back((uint32_t)tlist.size());
+          tlist.push_back((uint32_t)placed.size() - 1);
+          last_marker_end = off + r.out_len;
+        }
         so += r.out_len;
       }
       for (uint64_t b = 0; b < mp.out_len; b += kCrcBlock)
@@ -748,6 +807,7 @@ int gzgpu_create(gzgpu_ctx** out, const gzgpu_config* cfg) {
     if (cfg->lut_bits == 11 || cfg->lut_bits == 12) c->lut_bits = cfg->lut_bits;
     c->autotune = cfg->autotune != 0;
     c->ring = cfg->ring_history != 0;
+    if (cfg->ctas_per_sm == 3 || cfg->ctas_per_sm == 4) c->ctas_per_sm = cfg->ctas_per_sm;
   }
   if (cudaSetDevice(c->dev) != cudaSuccess) {
     delete c;

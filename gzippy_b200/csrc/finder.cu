@@ -1,7 +1,8 @@
 // finder.cu -- deflate block-boundary finder (K1) and chunk linking.
 //
-// One warp per speculative chunk searches [guess_bit, limit_bit) for the
-// first block-start candidate (predicate and search in finder_core.cuh).
+// Each speculative chunk searches [guess_bit, limit_bit) for its first
+// block-start candidate (predicate and search in finder_core.cuh) with the
+// warps of one CTA.
 #include <cstdint>
 
 #include "common.cuh"
@@ -10,18 +11,56 @@
 
 namespace gzgpu {
 
-__global__ void finder_kernel(const uint8_t* __restrict__ in, ChunkDesc* descs,
-                              const uint32_t* __restrict__ spec, uint32_t n_spec) {
-  const int lane = threadIdx.x & 31;
-  const uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (w >= n_spec) return;
-  ChunkDesc& d = descs[spec[w]];
-  uint64_t lo = 0, hi = 0;
-  bool have = warp_find_first(in, d.in_end, d.guess_bit, d.limit_bit, lane, lo, hi);
-  if (lane == 0) {
-    if (have) {
-      d.lo_bit = lo;
-      d.start_bit = hi;
+// One CTA per speculative chunk.  Its warps take the 1024-bit windows of
+// [guess_bit, limit_bit) round-robin, each window searched for its first
+// candidate (by start bit, so windows partition the candidates); a warp stops
+// as soon as a lower window has a hit, so the work is about the distance to
+// the first candidate, split over the CTA's warps.
+constexpr int kFinderWarps = 8;
+constexpr uint64_t kFinderWindow = 1024;
+
+__global__ void __launch_bounds__(32 * kFinderWarps)
+    finder_kernel(const uint8_t* __restrict__ in, ChunkDesc* descs,
+                  const uint32_t* __restrict__ spec, uint32_t n_spec) {
+  __shared__ unsigned long long best_win;
+  __shared__ uint64_t hit_lo[kFinderWarps], hit_hi[kFinderWarps], hit_win[kFinderWarps];
+  __shared__ uint16_t leaf_lut[4096];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (blockIdx.x >= n_spec) return;
+  for (int i = threadIdx.x; i < 4096; i += blockDim.x) leaf_lut[i] = (uint16_t)precode_leaves4(i);
+  ChunkDesc& d = descs[spec[blockIdx.x]];
+  const uint64_t from = d.guess_bit, to = d.limit_bit, nbytes = d.in_end;
+  if (threadIdx.x == 0) best_win = ~0ull;
+  if (lane == 0) hit_win[warp] = ~0ull;
+  __syncthreads();
+  const uint64_t n_win = to > from ? (to - from + kFinderWindow - 1) / kFinderWindow : 0;
+  for (uint64_t k = warp; k < n_win; k += kFinderWarps) {
+    if (k > *(volatile unsigned long long*)&best_win) break;
+    const uint64_t w0 = from + k * kFinderWindow;
+    const uint64_t w1 = min(w0 + kFinderWindow, to);
+    uint64_t lo = 0, hi = 0;
+    if (warp_find_first(in, nbytes, w0, w1, to, lane, lo, hi, leaf_lut)) {
+      if (lane == 0) {
+        hit_lo[warp] = lo;
+        hit_hi[warp] = hi;
+        hit_win[warp] = k;
+        atomicMin(&best_win, (unsigned long long)k);
+      }
+      break;
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint64_t bw = ~0ull;
+    int bwarp = -1;
+    for (int i = 0; i < kFinderWarps; i++)
+      if (hit_win[i] < bw) {
+        bw = hit_win[i];
+        bwarp = i;
+      }
+    if (bwarp >= 0) {
+      d.lo_bit = hit_lo[bwarp];
+      d.start_bit = hit_hi[bwarp];
       d.flags |= kChunkValid;
     } else {
       d.flags &= ~kChunkValid;
@@ -64,9 +103,7 @@ __global__ void link_kernel(ChunkDesc* descs, uint32_t n, uint32_t* work, uint32
 cudaError_t launch_finder(const uint8_t* in, ChunkDesc* descs, const uint32_t* spec,
                           uint32_t n_spec, cudaStream_t stream) {
   if (n_spec == 0) return cudaSuccess;
-  const int warps = 8;
-  uint32_t blocks = (n_spec + warps - 1) / warps;
-  finder_kernel<<<blocks, 32 * warps, 0, stream>>>(in, descs, spec, n_spec);
+  finder_kernel<<<n_spec, 32 * kFinderWarps, 0, stream>>>(in, descs, spec, n_spec);
   return cudaGetLastError();
 }
 

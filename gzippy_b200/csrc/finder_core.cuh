@@ -39,17 +39,52 @@ static __device__ __forceinline__ bool kraft_exact(uint32_t leaves, uint32_t gt1
   return leaves == (1u << 15);
 }
 
-// Full dynamic-header predicate at `bit`.  `base` = stream start byte,
-// `nbytes` = stream end byte (absolute).
-static __device__ __noinline__ bool dyn_candidate(const uint8_t* in, uint64_t nbytes, uint64_t bit) {
+// Bits [bit, bit + 96) of the stream as (lo64, hi32), from four aligned
+// 32-bit loads; bits at or past the stream end read 0 (the buffer is padded,
+// so the loads stay inside it).
+static __device__ __forceinline__ void load_bits96(const uint8_t* in, uint64_t nbytes,
+                                                   uint64_t bit, uint64_t& x, uint32_t& xh) {
+  const uint32_t* in32 = reinterpret_cast<const uint32_t*>(in);
+  const uint64_t wi = bit >> 5;
+  const uint32_t w0 = in32[wi], w1 = in32[wi + 1], w2 = in32[wi + 2], w3 = in32[wi + 3];
+  const int sh = (int)(bit & 31);
+  const uint64_t a = ((uint64_t)w1 << 32) | w0, b = ((uint64_t)w3 << 32) | w2;
+  x = sh ? (a >> sh) | (b << (64 - sh)) : a;
+  xh = (uint32_t)(b >> sh);
   const uint64_t nbits = nbytes * 8;
-  if (bit + 17 > nbits) return false;
+  if (bit + 96 > nbits) {
+    const uint64_t valid = nbits > bit ? nbits - bit : 0;
+    if (valid < 64) {
+      x &= valid ? (~0ull >> (64 - valid)) : 0;
+      xh = 0;
+    } else {
+      xh &= valid > 64 ? (0xFFFFFFFFu >> (96 - valid)) : 0;
+    }
+  }
+}
+
+// Leaf count of 4 precode lengths (3 bits each) packed in 12 bits: the
+// table of validate_precode (blockfinder_validation.rs:148-226).
+static __device__ __forceinline__ uint32_t precode_leaves4(uint32_t v) {
+  uint32_t s = 0;
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    uint32_t L = (v >> (3 * i)) & 7;
+    s += L ? 1u << (7 - L) : 0u;
+  }
+  return s;
+}
+
+// Rest of the dynamic-header predicate once the 13-bit filter and the
+// precode leaf count have passed: Kraft-exact precode, code lengths decode,
+// EOB present, Kraft-exact litlen and dist sets.
+static __device__ __noinline__ bool dyn_candidate_full(const uint8_t* in, uint64_t nbytes,
+                                                       uint64_t bit) {
+  const uint64_t nbits = nbytes * 8;
   uint32_t h = (uint32_t)peek_bits(in, nbytes, bit, 17);
-  if ((h & 1) || ((h >> 1) & 3) != 2 || ((h >> 3) & 31) > 29 || ((h >> 8) & 31) > 29) return false;
   int hlit = (h >> 3) & 31, hdist = (h >> 8) & 31, pc = ((h >> 13) & 15) + 4;
-  if (bit + 17 + 3 * pc > nbits) return false;
   uint64_t pbits = peek_bits(in, nbytes, bit + 17, 3 * pc);
-  uint32_t leaves7 = 0, leaves15 = 0, gt1 = 0;
+  uint32_t leaves15 = 0, gt1 = 0;
   uint8_t cl[19];
 #pragma unroll
   for (int i = 0; i < 19; i++) cl[i] = 0;
@@ -57,12 +92,10 @@ static __device__ __noinline__ bool dyn_candidate(const uint8_t* in, uint64_t nb
     uint32_t L = (uint32_t)(pbits >> (3 * i)) & 7;
     cl[f_cl_order[i]] = (uint8_t)L;
     if (L) {
-      leaves7 += 1u << (7 - L);
       leaves15 += 1u << (15 - L);
       gt1 += L > 1;
     }
   }
-  if (leaves7 != 128 && leaves7 != 64) return false;
   if (!kraft_exact(leaves15, gt1)) return false;
   // canonical precode tables
   uint16_t cnt[8], first[8], offs[8];
@@ -145,12 +178,42 @@ static __device__ __noinline__ bool dyn_candidate(const uint8_t* in, uint64_t nb
   return kraft_exact(lit_leaves, lit_gt1) && kraft_exact(dist_leaves, dist_gt1);
 }
 
+// Full dynamic-header predicate at `bit` (13-bit header filter, precode leaf
+// count via `leaf_lut`, then dyn_candidate_full).  `leaf_lut` is the 4096-entry
+// leaf-count table, or null to count arithmetically.
+static __device__ __forceinline__ bool dyn_candidate_fast(const uint8_t* in, uint64_t nbytes,
+                                                          uint64_t bit,
+                                                          const uint16_t* leaf_lut) {
+  if (bit + 17 > nbytes * 8) return false;
+  uint64_t x;
+  uint32_t xh;
+  load_bits96(in, nbytes, bit, x, xh);
+  const uint32_t h = (uint32_t)x;
+  if ((h & 1) || ((h >> 1) & 3) != 2 || ((h >> 3) & 31) > 29 || ((h >> 8) & 31) > 29) return false;
+  const int pc = ((h >> 13) & 15) + 4;
+  if (bit + 17 + 3 * pc > nbytes * 8) return false;
+  // precode bits [17, 17 + 3*pc) of the 96-bit window
+  uint64_t pb = (x >> 17) | ((uint64_t)xh << 47);
+  pb &= (1ull << (3 * pc)) - 1;
+  uint32_t leaves;
+  if (leaf_lut) {
+    leaves = leaf_lut[pb & 0xFFF] + leaf_lut[(pb >> 12) & 0xFFF] + leaf_lut[(pb >> 24) & 0xFFF] +
+             leaf_lut[(pb >> 36) & 0xFFF] + leaf_lut[pb >> 48];
+  } else {
+    leaves = precode_leaves4((uint32_t)(pb & 0xFFF)) + precode_leaves4((uint32_t)((pb >> 12) & 0xFFF)) +
+             precode_leaves4((uint32_t)((pb >> 24) & 0xFFF)) +
+             precode_leaves4((uint32_t)((pb >> 36) & 0xFFF)) + precode_leaves4((uint32_t)(pb >> 48));
+  }
+  if (leaves != 128 && leaves != 64) return false;
+  return dyn_candidate_full(in, nbytes, bit);
+}
+
 // Stored candidate test at byte offset `off` (find_uncompressed_blocks):
 // LEN == ~NLEN at the byte boundary, 3 zero header bits before it; the
 // candidate spans [byte_bit - zero_run, byte_bit - 3].
 static __device__ __forceinline__ bool stored_candidate(const uint8_t* in, uint64_t nbytes,
                                                         uint64_t off, uint64_t from, uint64_t to,
-                                                        uint64_t& lo, uint64_t& hi) {
+                                                        uint64_t hi_to, uint64_t& lo, uint64_t& hi) {
   uint32_t sz = in[off] | (in[off + 1] << 8) | ((uint32_t)in[off + 2] << 16) |
                 ((uint32_t)in[off + 3] << 24);
   if (((sz ^ (sz >> 16)) & 0xFFFF) != 0xFFFF) return false;
@@ -165,23 +228,26 @@ static __device__ __forceinline__ bool stored_candidate(const uint8_t* in, uint6
   lo = byte_bit - tz;
   hi = byte_bit - 3;
   uint32_t len = sz & 0xFFFF;
-  return lo >= from && hi < to && len != 0 && off + 4 + len <= nbytes;
+  return lo >= from && lo < to && hi < hi_to && len != 0 && off + 4 + len <= nbytes;
 }
 
 // First candidate in (bit_offset, seek_bit) order with bit_offset in
-// [from, to) of the stream ending at byte `nbytes`; all 32 lanes call it
-// together and get the same answer.  The range is walked in 1024-bit
+// [from, to) of the stream ending at byte `nbytes` (a stored candidate's
+// seek bit must also be below hi_to); all 32 lanes call it together and get
+// the same answer.  The range is walked in 1024-bit
 // windows; in each, lanes test 32 byte offsets (stored) or 32 bit offsets
 // (dynamic) per step and a ballot picks the lowest hit.  The first stored hit
 // in byte order is the smallest stored candidate, so the dynamic scan only
 // needs to reach it.
 static __device__ bool warp_find_first(const uint8_t* __restrict__ in, uint64_t nbytes,
-                                       uint64_t from, uint64_t to, int lane, uint64_t& out_lo,
-                                       uint64_t& out_hi) {
+                                       uint64_t from, uint64_t to, uint64_t hi_to, int lane,
+                                       uint64_t& out_lo, uint64_t& out_hi,
+                                       const uint16_t* leaf_lut = nullptr) {
   if (to > nbytes * 8) to = nbytes * 8;
+  if (hi_to > nbytes * 8) hi_to = nbytes * 8;
   bool have = false;
   uint64_t best_lo = 0, best_hi = 0;
-  const uint64_t until = nbytes >= 5 ? min((to + 7) / 8, nbytes - 4) : 0;
+  const uint64_t until = nbytes >= 5 ? min((hi_to + 7) / 8, nbytes - 4) : 0;
   uint64_t next_off = max((from + 3 + 7) / 8, (uint64_t)2);
   for (uint64_t w0 = from; w0 < to; w0 += 1024) {
     const uint64_t w1 = min(w0 + 1024, to);
@@ -190,7 +256,7 @@ static __device__ bool warp_find_first(const uint8_t* __restrict__ in, uint64_t 
     while (!have && next_off < off_end) {
       uint64_t off = next_off + lane;
       uint64_t lo = 0, hi = 0;
-      bool hit = off < off_end && stored_candidate(in, nbytes, off, from, to, lo, hi);
+      bool hit = off < off_end && stored_candidate(in, nbytes, off, from, to, hi_to, lo, hi);
       uint32_t m = __ballot_sync(0xFFFFFFFFu, hit);
       if (m) {
         int src = __ffs(m) - 1;
@@ -204,7 +270,7 @@ static __device__ bool warp_find_first(const uint8_t* __restrict__ in, uint64_t 
     const uint64_t lim = have ? min(w1, best_lo + 1) : w1;
     for (uint64_t p0 = w0; p0 < lim; p0 += 32) {
       uint64_t p = p0 + lane;
-      bool hit = p < lim && dyn_candidate(in, nbytes, p);
+      bool hit = p < lim && dyn_candidate_fast(in, nbytes, p, leaf_lut);
       uint32_t m = __ballot_sync(0xFFFFFFFFu, hit);
       if (m) {
         out_lo = out_hi = p0 + (__ffs(m) - 1);

@@ -95,16 +95,17 @@ struct alignas(16) RingSmem {
 };
 
 // ---------------------------------------------------------------------------
-// Bit reader over the register-staged input windows.
+// Bit reader over the register-staged input windows: a 128-bit bit window
+// (bb = bits 0..63, hi = bits 64..127), refilled to > 96 valid bits.
 // ---------------------------------------------------------------------------
 struct BitReader {
   const uint32_t* in32;
-  uint64_t win_base;  // word index of the current window
-  uint32_t win_cur;   // this lane's word of the current window
-  uint32_t win_next;  // this lane's word of the next window
-  uint64_t bb;        // bit buffer (LSB = next bit)
-  int bc;             // valid bits in bb
-  uint64_t wpos;      // word index of the next word to append to bb
+  uint64_t win_base;  // word index of the current input window
+  uint32_t win_cur;   // this lane's word of the current input window
+  uint32_t win_next;  // this lane's word of the next input window
+  uint64_t bb, hi;    // bit window (LSB = next bit)
+  int bc;             // valid bits in the window
+  uint64_t wpos;      // word index of the next word to append
   uint64_t limit_words;
 
   __device__ __forceinline__ void load_windows(uint64_t base, int lane) {
@@ -130,19 +131,41 @@ struct BitReader {
     uint64_t wi = bit >> 5;
     load_windows(wi & ~31ull, lane);
     bb = word(wi, lane) >> (bit & 31);
+    hi = 0;
     bc = 32 - (int)(bit & 31);
     wpos = wi + 1;
   }
+  __device__ __forceinline__ void append(uint32_t w) {
+    if (bc < 64) {
+      bb |= (uint64_t)w << bc;
+      if (bc > 32) hi |= (uint64_t)w >> (64 - bc);
+    } else {
+      hi |= (uint64_t)w << (bc - 64);
+    }
+    bc += 32;
+  }
   __device__ __forceinline__ void refill(int lane) {
-    if (bc <= 32) {
-      bb |= (uint64_t)word(wpos, lane) << bc;
-      bc += 32;
-      wpos++;
+    while (bc <= 96) append(word(wpos++, lane));
+  }
+  __device__ __forceinline__ void consume(int k) {  // 0 <= k < 64
+    if (k) {
+      bb = (bb >> k) | (hi << (64 - k));
+      hi >>= k;
+      bc -= k;
     }
   }
-  __device__ __forceinline__ void consume(int k) {
-    bb >>= k;
-    bc -= k;
+  __device__ __forceinline__ void consume_wide(int k) {  // 0 <= k < 128
+    if (k >= 64) {
+      bb = hi >> (k - 64);
+      hi = 0;
+      bc -= k;
+    } else {
+      consume(k);
+    }
+  }
+  // bits [i, i + 64) of the window, 0 <= i < 64
+  __device__ __forceinline__ uint64_t peek_at(int i) const {
+    return i ? (bb >> i) | (hi << (64 - i)) : bb;
   }
   __device__ __forceinline__ uint64_t pos() const { return wpos * 32 - (uint64_t)bc; }
   __device__ __forceinline__ bool overrun() const { return wpos > limit_words; }
@@ -460,6 +483,163 @@ __device__ bool ring_flush_tail(const uint16_t* ring, PageWriter& pw, const Page
 }
 
 // ---------------------------------------------------------------------------
+// Huffman block body, lane-parallel (page history).
+//
+// Every step, lane i decodes a whole symbol as if one started at bit i of the
+// window: the litlen code, its extra bits and, for a length, the distance
+// code and its extra bits (<= 48 bits).  The symbols that really start in the
+// first 32 bits form a chain 0 -> total(0) -> ... that a few warp shuffles
+// walk; literals of the chain are stored in parallel at their prefix-sum
+// output offsets, then the matches are copied in order, 32 entries per pass.
+// One step replaces ~4-6 dependent table lookups by one parallel lookup and
+// a shuffle per symbol.
+// ---------------------------------------------------------------------------
+constexpr uint32_t kStepMaxOut = 16 * 258 + 32;  // output bound of one step
+
+// Decode the symbol at bits [0, 48) of x with the full tables (long codes
+// included).  Returns packed info ([5:0] total bits, [7:6] kind, [31:16]
+// literal or length); *dist gets the distance; kind kKindBad if invalid.
+template <int LB>
+__device__ __forceinline__ uint32_t decode_symbol_full(uint64_t x, const Tables<LB>* T,
+                                                       uint32_t* dist) {
+  constexpr uint32_t LMASK = (1u << LB) - 1, DMASK = (1u << kDistBits) - 1;
+  uint32_t e = T->lit_lut[x & LMASK];
+  if ((e & 15) == 0)
+    e = slow_decode<LB>(x, T->lit_count, T->lit_first, T->lit_offs, T->lit_sorted, litlen_entry);
+  if (e == 0) return kKindBad << 6;
+  uint32_t L = e & 15, kind = (e >> 8) & 3, val = e >> 16, total = L;
+  if (kind == kKindLen) {
+    uint32_t xb = (e >> 4) & 15;
+    val += (uint32_t)(x >> L) & ((1u << xb) - 1);
+    uint32_t sh = L + xb;
+    uint64_t y = x >> sh;
+    uint32_t de = T->dist_lut[y & DMASK];
+    if ((de & 15) == 0)
+      de = slow_decode<kDistBits>(y, T->dist_count, T->dist_first, T->dist_offs, T->dist_sorted,
+                                  dist_entry);
+    if (de == 0 || ((de >> 8) & 3) == kKindBad) return kKindBad << 6;
+    uint32_t DL = de & 15, dxb = (de >> 4) & 15;
+    *dist = (de >> 16) + ((uint32_t)(y >> DL) & ((1u << dxb) - 1));
+    total = sh + DL + dxb;
+  }
+  return total | (kind << 6) | (val << 16);
+}
+
+template <int LB>
+__device__ int32_t huff_block_parallel(BitReader& br, const Tables<LB>* T, PageHist& ph,
+                                       const PagePool& pool, uint32_t cid, uint32_t gen,
+                                       uint64_t& o, uint64_t& guard, uint64_t& marker_end,
+                                       bool zero_window, uint64_t trunc_words, int lane) {
+  constexpr uint32_t LMASK = (1u << LB) - 1, DMASK = (1u << kDistBits) - 1;
+  for (;;) {
+    if (o >= guard) {
+      ph.advance(o);
+      if (!ph.ensure(pool, cid, gen, o + kStepMaxOut, lane)) return kPoolExhausted;
+      uint64_t pe = (ph.s + 1) << 16;  // end of the current page
+      guard = ph.next != kNoPage ? pe : pe - kStepMaxOut;
+    }
+    br.refill(lane);
+    if (br.overrun()) return br.wpos > trunc_words ? kTruncated : kOvershoot;
+    // lane-local decode of a symbol starting at bit `lane`
+    const uint64_t x = br.peek_at(lane);
+    uint32_t info, dinfo = 0;
+    {
+      uint32_t e = T->lit_lut[x & LMASK];
+      uint32_t L = e & 15, kind = (e >> 8) & 3, val = e >> 16, total = L;
+      uint32_t slow = L == 0;
+      if (!slow && kind == kKindLen) {
+        uint32_t xb = (e >> 4) & 15;
+        val += (uint32_t)(x >> L) & ((1u << xb) - 1);
+        uint32_t sh = L + xb;
+        uint64_t y = x >> sh;
+        uint32_t de = T->dist_lut[y & DMASK];
+        uint32_t DL = de & 15;
+        if (DL == 0 || ((de >> 8) & 3) == kKindBad) {
+          slow = 1;  // long or invalid distance code: resolved on the chain
+        } else {
+          uint32_t dxb = (de >> 4) & 15;
+          dinfo = (de >> 16) + ((uint32_t)(y >> DL) & ((1u << dxb) - 1));
+          total = sh + DL + dxb;
+        }
+      }
+      info = total | (kind << 6) | (slow << 8) | (val << 16);
+    }
+    // walk the chain of symbols that start in bits [0, 32)
+    uint32_t path = 0, p = 0;
+    bool eob = false;
+    while (p < 32) {
+      uint32_t ip = __shfl_sync(0xFFFFFFFFu, info, (int)p);
+      if (ip & 0x100) {
+        uint32_t dd = 0;
+        ip = decode_symbol_full<LB>(br.peek_at((int)p), T, &dd);
+        if (lane == (int)p) {
+          info = ip;
+          dinfo = dd;
+        }
+      }
+      uint32_t kind = (ip >> 6) & 3;
+      if (kind == kKindBad) return kBadDeflate;
+      path |= 1u << p;
+      p += ip & 63;
+      if (kind == kKindEob) {
+        eob = true;
+        break;
+      }
+    }
+    // output offsets: exclusive prefix sum of output lengths along the chain
+    const bool on = (path >> lane) & 1;
+    const uint32_t kind = (info >> 6) & 3;
+    const uint32_t olen = on ? (kind == kKindLit ? 1u : (kind == kKindLen ? (info >> 16) : 0u)) : 0u;
+    uint32_t incl = olen;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      uint32_t t = __shfl_up_sync(0xFFFFFFFFu, incl, d);
+      if (lane >= d) incl += t;
+    }
+    const uint32_t excl = incl - olen;
+    const uint32_t step_out = __shfl_sync(0xFFFFFFFFu, incl, 31);
+    if (on && kind == kKindLit) *ph.at(o + excl) = (uint16_t)(info >> 16);
+    uint32_t mm = __ballot_sync(0xFFFFFFFFu, on && kind == kKindLen);
+    while (mm) {
+      __syncwarp();
+      const int src = __ffs(mm) - 1;
+      mm &= mm - 1;
+      const uint32_t len = __shfl_sync(0xFFFFFFFFu, info >> 16, src);
+      const uint32_t dist = __shfl_sync(0xFFFFFFFFu, dinfo, src);
+      const uint64_t po = o + __shfl_sync(0xFFFFFFFFu, excl, src);
+      if ((uint64_t)dist > po + kWindow) return kBadDeflate;
+      // entry po+j = entry po-dist+(j mod dist); every source is older than po
+      const bool wrap = dist < len;
+      const uint32_t step_mod = wrap ? 32 % dist : 0;
+      uint32_t r = wrap ? (uint32_t)lane % dist : (uint32_t)lane;
+      for (uint32_t j0 = 0; j0 < len; j0 += 32) {
+        const uint32_t j = j0 + lane;
+        const bool act = j < len;
+        uint16_t v = 0;
+        if (act) {
+          const int64_t sp = (int64_t)po - (int64_t)dist + (int64_t)(wrap ? r : j);
+          if (sp >= 0) v = *ph.at((uint64_t)sp);
+          else v = zero_window ? 0 : (uint16_t)(kMarkerBase + kWindow + sp);
+          *ph.at(po + j) = v;
+        }
+        if (!zero_window) {
+          uint32_t m = __ballot_sync(0xFFFFFFFFu, act && v >= kMarkerBase);
+          if (m) marker_end = po + j0 + 32 - __clz(m);
+        }
+        if (wrap) {
+          r += step_mod;
+          if (r >= dist) r -= dist;
+        }
+      }
+    }
+    __syncwarp();
+    o += step_out;
+    br.consume_wide((int)p);
+    if (eob) return kOk;
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Decode one chunk.  kRing selects the history layout.
 // ---------------------------------------------------------------------------
 template <int LB, bool kRing>
@@ -487,9 +667,10 @@ __device__ int32_t decode_chunk(const uint8_t* __restrict__ in, const ChunkDesc&
 
   BitReader br;
   br.in32 = reinterpret_cast<const uint32_t*>(in);
-  const uint64_t trunc_words = (d.in_end * 8 + 31) / 32 + 2;
+  // the window reads up to 128 bits (4 words) ahead of the decode position
+  const uint64_t trunc_words = (d.in_end * 8 + 31) / 32 + 5;
   br.limit_words = trunc_words;
-  if (d.abort_bit != kNoStop && d.abort_bit / 32 + 2 < trunc_words) br.limit_words = d.abort_bit / 32 + 2;
+  if (d.abort_bit != kNoStop && d.abort_bit / 32 + 5 < trunc_words) br.limit_words = d.abort_bit / 32 + 5;
   br.seek(d.start_bit, lane);
   br.refill(lane);
 
@@ -563,8 +744,19 @@ __device__ int32_t decode_chunk(const uint8_t* __restrict__ in, const ChunkDesc&
     } else if (btype == 1 || btype == 2) {
       status = read_tables<LB>(br, btype, T, trunc_words, lane);
       if (status != kOk) break;
-      // Huffman-coded block body
-      for (;;) {
+      if (!kRing) {
+        status = huff_block_parallel<LB>(br, T, ph, pool, cid, gen, o, guard, marker_end,
+                                         zero_window, trunc_words, lane);
+        if (status != kOk) break;
+        n_blocks++;
+        if (bfinal) {
+          final_block = 1;
+          break;
+        }
+        continue;
+      }
+      // Huffman-coded block body (ring layout: serial decode)
+      if constexpr (kRing) for (;;) {
         if (kRing) {
           if (o - flushed >= kFlush && !ring_flush_full(ring, pw, pool, flushed, cid, gen, lane)) {
             status = kPoolExhausted;
@@ -737,7 +929,7 @@ __device__ __forceinline__ void work_loop(const uint8_t* __restrict__ in, ChunkD
       int32_t st = decode_chunk<LB, kRing>(in, d, &results[cid], cid, gen, ring, T, pool, lane);
       if (st == kOk || st == kPoolExhausted || !speculative || gen + 1 >= kMaxTries) break;
       uint64_t lo = 0, hi = 0;
-      if (!warp_find_first(in, d.in_end, d.lo_bit + 1, d.limit_bit, lane, lo, hi)) break;
+      if (!warp_find_first(in, d.in_end, d.lo_bit + 1, d.limit_bit, d.limit_bit, lane, lo, hi)) break;
       d.lo_bit = lo;
       d.start_bit = hi;
       if (lane == 0) {
@@ -768,8 +960,8 @@ __global__ void __launch_bounds__(32 * kRingWarps)
                       lane);
 }
 
-template <int LB>
-__global__ void __launch_bounds__(32 * kPageWarps, kPageMinBlocks)
+template <int LB, int MINB>
+__global__ void __launch_bounds__(32 * kPageWarps, MINB)
     inflate_pages_kernel(const uint8_t* __restrict__ in, ChunkDesc* __restrict__ descs,
                          ChunkResult* __restrict__ results, const uint32_t* __restrict__ work,
                          const uint32_t* __restrict__ n_work_ptr, uint32_t* work_counter,
@@ -786,10 +978,17 @@ size_t inflate_smem_bytes(bool ring) {
   return ring ? sizeof(RingSmem<LB>) * kRingWarps : sizeof(Tables<LB>) * kPageWarps;
 }
 
+// page kernel instance for `ctas` CTAs per SM (registers sized for it)
 template <int LB>
-cudaError_t launch_inflate(bool ring, const uint8_t* in, ChunkDesc* descs, ChunkResult* results,
-                           const uint32_t* work, const uint32_t* n_work, uint32_t* work_counter,
-                           const PagePool& pool, int blocks, cudaStream_t stream) {
+static const void* pages_kernel_fn(int ctas) {
+  return ctas >= 4 ? (const void*)inflate_pages_kernel<LB, 4> : (const void*)inflate_pages_kernel<LB, 3>;
+}
+
+template <int LB>
+cudaError_t launch_inflate(bool ring, int ctas, const uint8_t* in, ChunkDesc* descs,
+                           ChunkResult* results, const uint32_t* work, const uint32_t* n_work,
+                           uint32_t* work_counter, const PagePool& pool, int blocks,
+                           cudaStream_t stream) {
   size_t smem = inflate_smem_bytes<LB>(ring);
   cudaError_t e;
   if (ring) {
@@ -799,17 +998,21 @@ cudaError_t launch_inflate(bool ring, const uint8_t* in, ChunkDesc* descs, Chunk
     inflate_ring_kernel<LB><<<blocks, 32 * kRingWarps, smem, stream>>>(in, descs, results, work,
                                                                        n_work, work_counter, pool);
   } else {
-    e = cudaFuncSetAttribute(inflate_pages_kernel<LB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem);
+    const void* fn = pages_kernel_fn<LB>(ctas);
+    e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    inflate_pages_kernel<LB><<<blocks, 32 * kPageWarps, smem, stream>>>(in, descs, results, work,
-                                                                        n_work, work_counter, pool);
+    if (ctas >= 4)
+      inflate_pages_kernel<LB, 4><<<blocks, 32 * kPageWarps, smem, stream>>>(
+          in, descs, results, work, n_work, work_counter, pool);
+    else
+      inflate_pages_kernel<LB, 3><<<blocks, 32 * kPageWarps, smem, stream>>>(
+          in, descs, results, work, n_work, work_counter, pool);
   }
   return cudaGetLastError();
 }
 
 template <int LB>
-int inflate_blocks_per_sm(bool ring) {
+int inflate_blocks_per_sm(bool ring, int ctas) {
   int n = 0;
   size_t smem = inflate_smem_bytes<LB>(ring);
   if (ring) {
@@ -817,18 +1020,19 @@ int inflate_blocks_per_sm(bool ring) {
                          (int)smem);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, inflate_ring_kernel<LB>, 32 * kRingWarps, smem);
   } else {
-    cudaFuncSetAttribute(inflate_pages_kernel<LB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)smem);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, inflate_pages_kernel<LB>, 32 * kPageWarps, smem);
+    const void* fn = pages_kernel_fn<LB>(ctas);
+    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, 32 * kPageWarps, smem);
+    if (n > ctas) n = ctas;
   }
   return n;
 }
 
-#define GZGPU_INST(LB)                                                                        \
-  template size_t inflate_smem_bytes<LB>(bool);                                               \
-  template int inflate_blocks_per_sm<LB>(bool);                                               \
-  template cudaError_t launch_inflate<LB>(bool, const uint8_t*, ChunkDesc*, ChunkResult*,     \
-                                          const uint32_t*, const uint32_t*, uint32_t*,        \
+#define GZGPU_INST(LB)                                                                       \
+  template size_t inflate_smem_bytes<LB>(bool);                                              \
+  template int inflate_blocks_per_sm<LB>(bool, int);                                         \
+  template cudaError_t launch_inflate<LB>(bool, int, const uint8_t*, ChunkDesc*, ChunkResult*, \
+                                          const uint32_t*, const uint32_t*, uint32_t*,       \
                                           const PagePool&, int, cudaStream_t);
 GZGPU_INST(10)
 GZGPU_INST(11)

@@ -8,16 +8,18 @@ namespace gzgpu {
 
 constexpr int kRingWarps = 1;      // ring kernel: warps per CTA (64 KB ring each)
 constexpr int kPageWarps = 8;      // page kernel: warps per CTA (tables only)
-constexpr int kPageMinBlocks = 4;  // page kernel: CTAs per SM the registers are sized for
 constexpr int kDistBits = 8;       // distance LUT index bits
 
 template <int LB>
 size_t inflate_smem_bytes(bool ring);
+// page kernel: `ctas` (3 or 4) CTAs of kPageWarps warps per SM; registers are
+// sized for that many (80 or 64 per thread)
 template <int LB>
-int inflate_blocks_per_sm(bool ring);
+int inflate_blocks_per_sm(bool ring, int ctas);
 template <int LB>
-cudaError_t launch_inflate(bool ring, const uint8_t* in, ChunkDesc* descs, ChunkResult* results,
-                           const uint32_t* work, const uint32_t* n_work, uint32_t* work_counter,
-                           const PagePool& pool, int blocks, cudaStream_t stream);
+cudaError_t launch_inflate(bool ring, int ctas, const uint8_t* in, ChunkDesc* descs,
+                           ChunkResult* results, const uint32_t* work, const uint32_t* n_work,
+                           uint32_t* work_counter, const PagePool& pool, int blocks,
+                           cudaStream_t stream);
 
 }  // namespace gzgpu

@@ -47,8 +47,9 @@ __global__ void tail_literals_kernel(const PlacedChunk* __restrict__ placed, uin
   }
 }
 
-// one CTA per segment of the ordered tail-marker list (one segment per
-// stream); inside a segment, chunks are resolved strictly in order.
+// one CTA per run of the ordered tail-marker list: a run holds chunks whose
+// windows reach into each other's tails; runs (and streams) are independent.
+// Inside a run, chunks are resolved strictly in order.
 __global__ void tail_markers_kernel(const PlacedChunk* __restrict__ placed,
                                     const uint32_t* __restrict__ list,
                                     const uint32_t* __restrict__ seg_begin, uint32_t n_seg,

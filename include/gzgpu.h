@@ -53,6 +53,8 @@ typedef struct {
   int autotune;       /* 1 = choose chunk_bytes / lut_bits per job from the tuning table */
   int ring_history;   /* 1 = decode history in a shared-memory ring (3 warps/SM) instead
                          of the output pages in HBM (32 warps/SM, the default) */
+  int ctas_per_sm;    /* page-history decoder: 3 (24 warps/SM, 80 registers; default) or
+                         4 (32 warps/SM, 64 registers); 0 = default */
 } gzgpu_config;
 
 typedef struct {
