@@ -259,7 +259,8 @@ class Context:
 
     DESC_DTYPE = np.dtype([("start_bit", "<u8"), ("lo_bit", "<u8"), ("stop_lo", "<u8"),
                            ("guess_bit", "<u8"), ("limit_bit", "<u8"), ("in_end", "<u8"),
-                           ("abort_bit", "<u8"), ("flags", "<u4"), ("stream", "<u4")])
+                           ("abort_bit", "<u8"), ("flags", "<u4"), ("stream", "<u4"),
+                           ("next", "<u4"), ("pad", "<u4")])
     RESULT_DTYPE = np.dtype([("end_bit", "<u8"), ("out_len", "<u8"), ("marker_end", "<u8"),
                              ("last_page", "<u4"), ("prev_page", "<u4"), ("n_pages", "<u4"),
                              ("n_blocks", "<u4"), ("status", "<i4"), ("final_block", "<i4"),

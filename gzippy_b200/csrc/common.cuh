@@ -54,7 +54,11 @@ struct ChunkDesc {
   uint64_t abort_bit;  // a speculative chunk gives up past this bit (kNoStop = never)
   uint32_t flags;
   uint32_t stream;     // stream id
+  uint32_t next;       // index of the next valid chunk of the stream (kNoChunk = none)
+  uint32_t pad;
 };
+constexpr uint32_t kNoChunk = 0xFFFFFFFFu;
+constexpr int kMaxExtends = 4;  // phantom successors a chunk decodes through
 
 struct ChunkResult {
   uint64_t end_bit;     // bit where decoding stopped

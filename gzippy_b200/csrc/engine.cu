@@ -440,6 +440,7 @@ int gzgpu_ctx::run(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R) 
     d.in_end = S[w.stream].off + S[w.stream].len;
     d.flags = flags | kChunkValid;
     d.stream = w.stream;
+    d.next = kNoChunk;
     uint32_t id = (uint32_t)(hd.size() + repairs.size());
     repairs.push_back(d);
     repair_owner.push_back(w.stream);
@@ -532,20 +533,30 @@ int gzgpu_ctx::run(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R) 
         w.cur = -1;
         continue;
       }
+      // accept the chunk whose start range holds the confirmed end; discard
+      // the starts the end passed (phantom speculative starts, and member
+      // candidates that lay inside this member's data)
       const uint64_t e = r.end_bit;
+      auto first_bit = [&](uint32_t k) { return is_mf(k) ? hd[k].limit_bit * 8 : hd[k].lo_bit; };
       uint32_t j = w.j;
-      while (j < w.c1 && !is_valid(j)) j++;
-      if (j < w.c1 && !is_mf(j) && e >= hd[j].lo_bit && e <= hd[j].start_bit && hr[j].status == kOk) {
+      bool accepted = false;
+      while (j < w.c1) {
+        if (!is_valid(j)) {
+          j++;
+          continue;
+        }
+        if (!is_mf(j) && e >= hd[j].lo_bit && e <= hd[j].start_bit && hr[j].status == kOk) {
+          accepted = true;
+          break;
+        }
+        if (first_bit(j) > e) break;
+        n_rejected++;
+        j++;
+      }
+      if (accepted) {
         w.cur = (int32_t)j;
         w.j = j + 1;
         continue;
-      }
-      // discard starts the confirmed end passed: speculative candidates and
-      // member candidates that lay inside this member's data
-      auto first_bit = [&](uint32_t k) { return is_mf(k) ? hd[k].limit_bit * 8 : hd[k].lo_bit; };
-      while (j < w.c1 && (!is_valid(j) || first_bit(j) <= e)) {
-        if (is_valid(j)) n_rejected++;
-        j++;
       }
       w.j = j;
       uint64_t stop = j < w.c1 ? first_bit(j) : kNoStop;
@@ -1101,6 +1112,7 @@ int gzgpu_debug_decode(gzgpu_ctx* c, const uint8_t* in, size_t in_len, const uin
     d[i].start_bit = d[i].lo_bit = d[i].guess_bit = d[i].limit_bit = start[i];
     d[i].stop_lo = stop[i];
     d[i].abort_bit = kNoStop;
+    d[i].next = kNoChunk;
     d[i].in_end = in_len;
     d[i].flags = kChunkValid | (member_first[i] ? kChunkMemberFirst : 0u);
     wl[i] = (uint32_t)i;

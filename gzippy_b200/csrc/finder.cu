@@ -81,6 +81,7 @@ __global__ void link_kernel(ChunkDesc* descs, uint32_t n, uint32_t* work, uint32
   ChunkDesc& d = descs[i];
   if (!(d.flags & kChunkValid)) return;
   uint64_t stop = kNoStop;
+  uint32_t next = kNoChunk;
   for (uint32_t j = i + 1; j < n; j++) {
     uint32_t f = descs[j].flags;
     if (descs[j].stream != d.stream) break;
@@ -88,14 +89,17 @@ __global__ void link_kernel(ChunkDesc* descs, uint32_t n, uint32_t* work, uint32
       // a member candidate (limit_bit = its header byte): a real one follows
       // the BFINAL block, a false one lies inside this member's data
       stop = descs[j].limit_bit * 8;
+      next = j;
       break;
     }
     if (f & kChunkValid) {
       stop = descs[j].lo_bit;
+      next = j;
       break;
     }
   }
   d.stop_lo = stop;
+  d.next = next;
   d.abort_bit = (stop != kNoStop && !(d.flags & kChunkMemberFirst)) ? stop + slack : kNoStop;
   work[atomicAdd(n_work, 1u)] = i;
 }

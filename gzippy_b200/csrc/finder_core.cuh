@@ -20,17 +20,18 @@ namespace gzgpu {
 
 static __constant__ uint8_t f_cl_order[19] = {16, 17, 18, 0, 8, 7, 9, 6, 10, 5, 11, 4, 12, 3, 13, 2, 14, 1, 15};
 
-// bits [bit, bit+k) of the input, k <= 57; bytes at or past `nbytes` read 0
+// bits [bit, bit+k) of the input, k <= 57; bits at or past the stream end
+// (byte `nbytes`) read 0.  Three aligned 32-bit loads (the buffer is padded).
 static __device__ __forceinline__ uint64_t peek_bits(const uint8_t* in, uint64_t nbytes, uint64_t bit,
-                                              int k) {
-  uint64_t byte = bit >> 3;
-  uint64_t v = 0;
-#pragma unroll
-  for (int i = 0; i < 8; i++) {
-    uint64_t b = byte + i;
-    v |= (uint64_t)(b < nbytes ? in[b] : 0) << (8 * i);
-  }
-  return (v >> (bit & 7)) & ((1ull << k) - 1);
+                                                     int k) {
+  const uint32_t* in32 = reinterpret_cast<const uint32_t*>(in);
+  const uint64_t wi = bit >> 5;
+  const int sh = (int)(bit & 31);
+  const uint64_t a = ((uint64_t)in32[wi + 1] << 32) | in32[wi];
+  uint64_t v = (a >> sh) | (sh ? (uint64_t)in32[wi + 2] << (64 - sh) : 0);
+  uint64_t avail = nbytes * 8 > bit ? nbytes * 8 - bit : 0;
+  int kk = avail < (uint64_t)k ? (int)avail : k;
+  return kk ? v & (~0ull >> (64 - kk)) : 0;
 }
 
 // Kraft equality over 15-bit leaves, or a single one-bit code.

@@ -129,7 +129,7 @@ struct BitReader {
   }
   __device__ __forceinline__ void seek(uint64_t bit, int lane) {
     uint64_t wi = bit >> 5;
-    load_windows(wi & ~31ull, lane);
+    if (wi < win_base || wi >= win_base + 32) load_windows(wi & ~31ull, lane);
     bb = word(wi, lane) >> (bit & 31);
     hi = 0;
     bc = 32 - (int)(bit & 31);
@@ -525,23 +525,63 @@ __device__ __forceinline__ uint32_t decode_symbol_full(uint64_t x, const Tables<
   return total | (kind << 6) | (val << 16);
 }
 
+// Page of a position relative to the start of page seq s: prev / cur / next.
+__device__ __forceinline__ uint16_t* page_addr(const PageHist& ph, int32_t rel) {
+  const uint32_t pg = rel < 0 ? ph.prev : (rel < (int32_t)kPageEntries ? ph.cur : ph.next);
+  return ph.data + (size_t)pg * kPageEntries + ((uint32_t)rel & (kPageEntries - 1));
+}
+
 template <int LB>
 __device__ int32_t huff_block_parallel(BitReader& br, const Tables<LB>* T, PageHist& ph,
                                        const PagePool& pool, uint32_t cid, uint32_t gen,
                                        uint64_t& o, uint64_t& guard, uint64_t& marker_end,
                                        bool zero_window, uint64_t trunc_words, int lane) {
   constexpr uint32_t LMASK = (1u << LB) - 1, DMASK = (1u << kDistBits) - 1;
+  uint64_t pos = br.pos();
+  int32_t status = kOk;
   for (;;) {
     if (o >= guard) {
       ph.advance(o);
-      if (!ph.ensure(pool, cid, gen, o + kStepMaxOut, lane)) return kPoolExhausted;
+      if (!ph.ensure(pool, cid, gen, o + kStepMaxOut, lane)) {
+        status = kPoolExhausted;
+        break;
+      }
       uint64_t pe = (ph.s + 1) << 16;  // end of the current page
       guard = ph.next != kNoPage ? pe : pe - kStepMaxOut;
     }
-    br.refill(lane);
-    if (br.overrun()) return br.wpos > trunc_words ? kTruncated : kOvershoot;
-    // lane-local decode of a symbol starting at bit `lane`
-    const uint64_t x = br.peek_at(lane);
+    // the step's 128 bits, from the register-staged input words
+    // (the header reader's read-ahead may have moved the staging past w0)
+    const uint64_t w0 = pos >> 5;
+    if (w0 < br.win_base || w0 + 3 >= br.win_base + 64) {
+      if (w0 >= br.win_base && w0 < br.win_base + 64) {
+        br.win_base += 32;
+        br.win_cur = br.win_next;
+        br.win_next = br.in32[br.win_base + 32 + lane];
+      } else {
+        br.load_windows(w0 & ~31ull, lane);
+      }
+    }
+    if (w0 + 4 > br.limit_words) {
+      status = w0 + 4 > trunc_words ? kTruncated : kOvershoot;
+      break;
+    }
+    uint32_t W[4];
+    {
+      const uint32_t rel = (uint32_t)(w0 - br.win_base);
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        const uint32_t r = rel + k;
+        const uint32_t a = __shfl_sync(0xFFFFFFFFu, br.win_cur, r & 31);
+        const uint32_t b2 = __shfl_sync(0xFFFFFFFFu, br.win_next, r & 31);
+        W[k] = r < 32 ? a : b2;
+      }
+    }
+    // lane-local decode of a symbol starting at bit `lane` of the step
+    const uint32_t t = (uint32_t)(pos & 31) + lane;  // 0..62
+    const uint32_t wa = t >> 5, bsh = t & 31;
+    const uint64_t lo64 = wa ? ((uint64_t)W[2] << 32 | W[1]) : ((uint64_t)W[1] << 32 | W[0]);
+    const uint32_t hi32 = wa ? W[3] : W[2];
+    const uint64_t x = bsh ? (lo64 >> bsh) | ((uint64_t)hi32 << (64 - bsh)) : lo64;
     uint32_t info, dinfo = 0;
     {
       uint32_t e = T->lit_lut[x & LMASK];
@@ -564,28 +604,54 @@ __device__ int32_t huff_block_parallel(BitReader& br, const Tables<LB>* T, PageH
       }
       info = total | (kind << 6) | (slow << 8) | (val << 16);
     }
+    // successor of a symbol starting here; 128 + lane stops the walk at a
+    // symbol that needs the full tables, ends the block or is invalid
+    // (chain positions stay below 32 + 48)
+    const uint32_t kind0 = (info >> 6) & 3;
+    uint32_t nxt = ((info & 0x100) || kind0 >= kKindEob) ? 128u + lane : lane + (info & 63);
     // walk the chain of symbols that start in bits [0, 32)
     uint32_t path = 0, p = 0;
     bool eob = false;
-    while (p < 32) {
-      uint32_t ip = __shfl_sync(0xFFFFFFFFu, info, (int)p);
-      if (ip & 0x100) {
-        uint32_t dd = 0;
-        ip = decode_symbol_full<LB>(br.peek_at((int)p), T, &dd);
-        if (lane == (int)p) {
-          info = ip;
-          dinfo = dd;
-        }
-      }
-      uint32_t kind = (ip >> 6) & 3;
-      if (kind == kKindBad) return kBadDeflate;
-      path |= 1u << p;
-      p += ip & 63;
-      if (kind == kKindEob) {
-        eob = true;
-        break;
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      if (p < 32) {
+        path |= 1u << p;
+        p = __shfl_sync(0xFFFFFFFFu, nxt, p & 31);
       }
     }
+    while (p < 32 || p >= 128) {
+      if (p >= 128) {
+        const uint32_t sl = p - 128;  // on the path already
+        uint32_t ip = __shfl_sync(0xFFFFFFFFu, info, (int)sl);
+        if (ip & 0x100) {
+          uint32_t dd = 0;
+          // bits [sl, sl + 64) of the step
+          const uint32_t ts = (uint32_t)(pos & 31) + sl;
+          const uint32_t was = ts >> 5, bs = ts & 31;
+          const uint64_t l64 = was ? ((uint64_t)W[2] << 32 | W[1]) : ((uint64_t)W[1] << 32 | W[0]);
+          const uint32_t h32 = was ? W[3] : W[2];
+          ip = decode_symbol_full<LB>(bs ? (l64 >> bs) | ((uint64_t)h32 << (64 - bs)) : l64, T, &dd);
+          if (lane == (int)sl) {
+            info = ip;
+            dinfo = dd;
+          }
+        }
+        const uint32_t kd = (ip >> 6) & 3;
+        if (kd == kKindBad) {
+          status = kBadDeflate;
+          break;
+        }
+        p = sl + (ip & 63);
+        if (kd == kKindEob) {
+          eob = true;
+          break;
+        }
+        continue;
+      }
+      path |= 1u << p;
+      p = __shfl_sync(0xFFFFFFFFu, nxt, p & 31);
+    }
+    if (status != kOk) break;
     // output offsets: exclusive prefix sum of output lengths along the chain
     const bool on = (path >> lane) & 1;
     const uint32_t kind = (info >> 6) & 3;
@@ -593,12 +659,13 @@ __device__ int32_t huff_block_parallel(BitReader& br, const Tables<LB>* T, PageH
     uint32_t incl = olen;
 #pragma unroll
     for (int d = 1; d < 32; d <<= 1) {
-      uint32_t t = __shfl_up_sync(0xFFFFFFFFu, incl, d);
-      if (lane >= d) incl += t;
+      uint32_t tt = __shfl_up_sync(0xFFFFFFFFu, incl, d);
+      if (lane >= d) incl += tt;
     }
     const uint32_t excl = incl - olen;
     const uint32_t step_out = __shfl_sync(0xFFFFFFFFu, incl, 31);
-    if (on && kind == kKindLit) *ph.at(o + excl) = (uint16_t)(info >> 16);
+    const int32_t orel = (int32_t)(o - (ph.s << 16));  // o within page seq s
+    if (on && kind == kKindLit) *page_addr(ph, orel + (int32_t)excl) = (uint16_t)(info >> 16);
     uint32_t mm = __ballot_sync(0xFFFFFFFFu, on && kind == kKindLen);
     while (mm) {
       __syncwarp();
@@ -606,25 +673,34 @@ __device__ int32_t huff_block_parallel(BitReader& br, const Tables<LB>* T, PageH
       mm &= mm - 1;
       const uint32_t len = __shfl_sync(0xFFFFFFFFu, info >> 16, src);
       const uint32_t dist = __shfl_sync(0xFFFFFFFFu, dinfo, src);
-      const uint64_t po = o + __shfl_sync(0xFFFFFFFFu, excl, src);
-      if ((uint64_t)dist > po + kWindow) return kBadDeflate;
+      const uint32_t mo = __shfl_sync(0xFFFFFFFFu, excl, src);
+      if ((uint64_t)dist > o + mo + kWindow) {
+        status = kBadDeflate;
+        break;
+      }
       // entry po+j = entry po-dist+(j mod dist); every source is older than po
+      const int32_t prel = orel + (int32_t)mo;  // copy start, page-relative
       const bool wrap = dist < len;
       const uint32_t step_mod = wrap ? 32 % dist : 0;
       uint32_t r = wrap ? (uint32_t)lane % dist : (uint32_t)lane;
+      // a source before the chunk's first entry is a window marker (or zero)
+      const int64_t before = (int64_t)(o + mo) - (int64_t)dist;  // chunk position of source j=0
       for (uint32_t j0 = 0; j0 < len; j0 += 32) {
         const uint32_t j = j0 + lane;
         const bool act = j < len;
         uint16_t v = 0;
         if (act) {
-          const int64_t sp = (int64_t)po - (int64_t)dist + (int64_t)(wrap ? r : j);
-          if (sp >= 0) v = *ph.at((uint64_t)sp);
-          else v = zero_window ? 0 : (uint16_t)(kMarkerBase + kWindow + sp);
-          *ph.at(po + j) = v;
+          const uint32_t sj = wrap ? r : j;
+          if (before + (int64_t)sj >= 0) {
+            v = *page_addr(ph, prel - (int32_t)dist + (int32_t)sj);
+          } else {
+            v = zero_window ? 0 : (uint16_t)(kMarkerBase + kWindow + before + sj);
+          }
+          *page_addr(ph, prel + (int32_t)j) = v;
         }
         if (!zero_window) {
           uint32_t m = __ballot_sync(0xFFFFFFFFu, act && v >= kMarkerBase);
-          if (m) marker_end = po + j0 + 32 - __clz(m);
+          if (m) marker_end = o + mo + j0 + 32 - __clz(m);
         }
         if (wrap) {
           r += step_mod;
@@ -632,20 +708,30 @@ __device__ int32_t huff_block_parallel(BitReader& br, const Tables<LB>* T, PageH
         }
       }
     }
+    if (status != kOk) break;
     __syncwarp();
     o += step_out;
-    br.consume_wide((int)p);
-    if (eob) return kOk;
+    pos += p;
+    if (eob) break;
   }
+  br.seek(pos, lane);
+  br.refill(lane);
+  return status;
 }
 
 // ---------------------------------------------------------------------------
 // Decode one chunk.  kRing selects the history layout.
 // ---------------------------------------------------------------------------
+// start bit a predecessor must reach to hand over to chunk k
+__device__ __forceinline__ uint64_t handover_bit(const ChunkDesc& k) {
+  return (k.flags & kChunkMemberFirst) ? k.limit_bit * 8 : k.lo_bit;
+}
+
 template <int LB, bool kRing>
-__device__ int32_t decode_chunk(const uint8_t* __restrict__ in, const ChunkDesc& d,
-                                ChunkResult* res, uint32_t cid, uint32_t gen, uint16_t* ring,
-                                Tables<LB>* T, const PagePool& pool, int lane) {
+__device__ int32_t decode_chunk(const uint8_t* __restrict__ in, ChunkDesc d,
+                                const ChunkDesc* descs, ChunkResult* res, uint32_t cid,
+                                uint32_t gen, uint16_t* ring, Tables<LB>* T,
+                                const PagePool& pool, int lane) {
   const bool zero_window = (d.flags & kChunkMemberFirst) != 0;
   if (kRing) {
     // seed the ring: zeros for a member start, marker values otherwise
@@ -671,6 +757,7 @@ __device__ int32_t decode_chunk(const uint8_t* __restrict__ in, const ChunkDesc&
   const uint64_t trunc_words = (d.in_end * 8 + 31) / 32 + 5;
   br.limit_words = trunc_words;
   if (d.abort_bit != kNoStop && d.abort_bit / 32 + 5 < trunc_words) br.limit_words = d.abort_bit / 32 + 5;
+  br.load_windows((d.start_bit >> 5) & ~31ull, lane);
   br.seek(d.start_bit, lane);
   br.refill(lane);
 
@@ -684,9 +771,28 @@ __device__ int32_t decode_chunk(const uint8_t* __restrict__ in, const ChunkDesc&
   // page-history fast path: positions below `guard` need no page work
   uint64_t guard = 0;
 
+  int extends = 0;
+  const uint64_t slack = d.abort_bit != kNoStop ? d.abort_bit - d.stop_lo : 0;
   for (;;) {
     uint64_t bitpos = br.pos();
-    if (bitpos >= d.stop_lo) break;
+    if (bitpos >= d.stop_lo) {
+      // A block boundary past the successor's start range means that start
+      // was a phantom: decode on to the start after it (the consumer's
+      // re-decode from the confirmed boundary, chunk_fetcher.rs:855).
+      if (d.next == kNoChunk || extends >= kMaxExtends) break;
+      const ChunkDesc nx = descs[d.next];
+      if ((nx.flags & kChunkMemberFirst) || bitpos <= nx.start_bit) break;
+      if (nx.next == kNoChunk) {
+        d.stop_lo = kNoStop;
+        d.abort_bit = kNoStop;
+      } else {
+        d.stop_lo = handover_bit(descs[nx.next]);
+        if (d.abort_bit != kNoStop) d.abort_bit = d.stop_lo + slack;
+      }
+      d.next = nx.next;
+      extends++;
+      if (bitpos >= d.stop_lo) continue;
+    }
     if (bitpos > d.abort_bit) {
       status = kOvershoot;
       break;
@@ -926,7 +1032,8 @@ __device__ __forceinline__ void work_loop(const uint8_t* __restrict__ in, ChunkD
     if (lane == 0) asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
     const bool speculative = !(d.flags & kChunkMemberFirst) && d.limit_bit > d.lo_bit;
     for (uint32_t gen = 0;; gen++) {
-      int32_t st = decode_chunk<LB, kRing>(in, d, &results[cid], cid, gen, ring, T, pool, lane);
+      int32_t st = decode_chunk<LB, kRing>(in, d, descs, &results[cid], cid, gen, ring, T, pool,
+                                           lane);
       if (st == kOk || st == kPoolExhausted || !speculative || gen + 1 >= kMaxTries) break;
       uint64_t lo = 0, hi = 0;
       if (!warp_find_first(in, d.in_end, d.lo_bit + 1, d.limit_bit, d.limit_bit, lane, lo, hi)) break;

@@ -133,8 +133,8 @@ int gzgpu_debug_decode(gzgpu_ctx *ctx, const uint8_t *in, size_t in_len, const u
                        size_t cap_per, uint64_t *res);
 
 /* gzgpu_debug_last_chunks: the chunk table of the last job.  descs holds
- * n records of 64 bytes (start_bit, lo_bit, stop_lo, guess_bit, limit_bit,
- * in_end, abort_bit as u64; flags, stream as u32); results n records of 72
+ * n records of 72 bytes (start_bit, lo_bit, stop_lo, guess_bit, limit_bit,
+ * in_end, abort_bit as u64; flags, stream, next, pad as u32); results n records of 72
  * bytes (end_bit, out_len, marker_end as u64; last_page, prev_page, n_pages,
  * n_blocks as u32; status, final_block as i32; t_start, t_end as u64 device
  * nanoseconds; gen as u32 + 4 pad bytes: 72 bytes).  *n = records available (copies min(cap, *n)). */

@@ -1105,20 +1105,25 @@ int orc_decompress_chunked(const uint8_t *in, size_t n, size_t chunk_bytes, int 
       }
       if (cur->r.final_block) break;
       uint64_t e = cur->r.end_bit;
-      while (j < nc && !ch[j].valid) j++;
-      if (j < nc && !ch[j].member_first && e >= ch[j].lo && e <= ch[j].hi &&
-          ch[j].r.status == ORC_OK) {
+#define FIRST_BIT(k) (ch[k].member_first ? mem[ch[k].member].start * 8 : ch[k].lo)
+      int accepted = 0;
+      while (j < nc) {
+        if (!ch[j].valid) { j++; continue; }
+        if (!ch[j].member_first && e >= ch[j].lo && e <= ch[j].hi && ch[j].r.status == ORC_OK) {
+          accepted = 1;
+          break;
+        }
+        if (FIRST_BIT(j) > e) break;
+        st->n_spec_rejected++;
+        j++;
+      }
+      if (accepted) {
         cur = &ch[j++];
         continue;
       }
       if (cur->r.out_len == 0 && cur->r.n_blocks == 0 && cur->lo == e && cur != &ch[j - 1]) {
         status = ORC_BAD_DEFLATE; /* no progress */
         break;
-      }
-#define FIRST_BIT(k) (ch[k].member_first ? mem[ch[k].member].start * 8 : ch[k].lo)
-      while (j < nc && (!ch[j].valid || FIRST_BIT(j) <= e)) {
-        if (ch[j].valid) st->n_spec_rejected++;
-        j++;
       }
       uint64_t stop = j < nc ? FIRST_BIT(j) : ~0ull;
 #undef FIRST_BIT
