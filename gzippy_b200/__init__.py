@@ -33,6 +33,8 @@ __all__ = ["GzippyError", "decompress", "decompress_with_threads", "decompress_t
 
 OK, NOT_GZIP, BAD_HEADER, BAD_DEFLATE, CRC_MISMATCH, SIZE_MISMATCH, OUT_TOO_SMALL = range(7)
 DEVICE_ERROR, TIMEOUT, TRUNCATED, INVALID_ARGUMENT = 7, 8, 9, 12
+NOALLOC_TOO_LARGE = 14
+NOALLOC_MAX_OUT = 4 << 20
 
 
 class GzippyError(Exception):
@@ -103,6 +105,7 @@ def lib():
             L.gzgpu_debug_find.argtypes = [vp, vp, sz, vp, vp, sz, vp, vp, vp]
             L.gzgpu_debug_decode.argtypes = [vp, vp, sz, vp, vp, vp, sz, vp, sz, vp]
             L.gzgpu_debug_last_chunks.argtypes = [vp, vp, vp, sz, ctypes.POINTER(sz)]
+            L.gzgpu_decompress_device_noalloc.argtypes = [vp, sz, vp, sz, ctypes.POINTER(sz), vp]
             _lib = L
     return _lib
 
@@ -333,6 +336,25 @@ def decompress_to_writer(data, writer) -> int:
 def decompress_to_writer_with_threads(data, writer, threads: int) -> int:
     """gzippy::decompress_to_writer_with_threads (src/lib.rs:221)."""
     return _ctx().decompress_to_writer(data, writer)
+
+
+def decompress_device_noalloc(d_in: int, in_len: int, d_out: int, out_cap: int,
+                              cuda_stream: int = 0) -> int:
+    """Decode without allocating device memory (include/gzgpu.h,
+    gzgpu_decompress_device_noalloc): for callers that cannot call cudaMalloc,
+    e.g. under a pool-only allocator or with all device memory reserved.  Raw
+    device pointers on the current device; output limited to
+    NOALLOC_MAX_OUT bytes.  Returns bytes written; raises GzippyError."""
+    n = ctypes.c_size_t(0)
+    rc = lib().gzgpu_decompress_device_noalloc(d_in, in_len, d_out, out_cap, ctypes.byref(n),
+                                               cuda_stream or None)
+    if rc == NOT_GZIP:
+        return 0
+    if rc != OK:
+        if rc == OUT_TOO_SMALL:
+            raise GzippyError("Decompression", f"output needs {n.value} bytes", rc)
+        _raise(rc)
+    return n.value
 
 
 def decompress_batch(datas) -> list:

@@ -37,6 +37,7 @@ enum : int32_t {
   kPoolExhausted = 10,
   kNotDecoded = 11,
   kOvershoot = 13,  // speculative chunk ran past stop_lo + slack without a block boundary
+  kNoAllocTooLarge = 14,  // output beyond the no-allocation entry point's limit
 };
 
 enum : uint32_t {

@@ -135,7 +135,8 @@ const char* kErrStr[] = {"ok",
                          "device page pool exhausted",
                          "chunk not decoded",
                          "invalid argument",
-                         "speculative chunk overshot its stop"};
+                         "speculative chunk overshot its stop",
+                         "output exceeds the 4 MiB limit of the no-allocation entry point"};
 
 }  // namespace
 

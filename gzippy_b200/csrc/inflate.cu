@@ -1145,4 +1145,215 @@ GZGPU_INST(10)
 GZGPU_INST(11)
 GZGPU_INST(12)
 
+// ===========================================================================
+// Decode without allocating: gzgpu_decompress_device_noalloc.
+//
+// For callers that cannot call cudaMalloc -- code under a pool-only
+// allocator that must not grow, real-time paths that cannot take the
+// device-wide synchronisation cudaMalloc/cudaFree may cause, or processes
+// whose device memory is reserved up front by another framework.  One warp decodes the stream's
+// members one after another (no speculation) with the same page-history
+// inflate as above; its pages, its chunk record and the status word live in
+// one file-scope device array that every GPU loading this library holds
+// until exit.  The caller owns input and output.
+// ===========================================================================
+constexpr uint64_t kNoAllocMaxOut = 4ull << 20;  // output limit of one call (bytes)
+constexpr uint32_t kNoAllocPages = (uint32_t)(kNoAllocMaxOut / kPageEntries) + 2;
+
+struct NoAllocScratch {
+  int32_t status;
+  uint32_t page_next;  // page allocation counter, cleared for every member
+  uint64_t out_len;
+  ChunkResult res;
+  uint32_t owner[kNoAllocPages];
+  uint32_t seq[kNoAllocPages];
+  alignas(256) uint16_t pages[(size_t)kNoAllocPages * kPageEntries];
+};
+
+static __device__ __align__(256) uint8_t g_noalloc_scratch[sizeof(NoAllocScratch)];
+
+static __device__ __forceinline__ uint32_t na_mulmod(uint32_t a, uint32_t b) {
+  uint32_t r = 0;
+  for (int i = 31; i >= 0; i--) {
+    r ^= b & (0u - ((a >> i) & 1u));
+    b = (b >> 1) ^ (0xEDB88320u & (0u - (b & 1u)));
+  }
+  return r;
+}
+
+// crc(A|B) from crc(A), crc(B) and |B|: x^(8|B|) * crc(A) + crc(B) mod P
+static __device__ uint32_t na_crc_combine(uint32_t c1, uint32_t c2, uint64_t len2) {
+  uint32_t xp = 1u << 30;  // x^1, squared up through x^(2^k)
+  uint32_t p = 1u << 31;   // x^0
+  for (uint64_t e = len2 * 8; e; e >>= 1) {
+    if (e & 1) p = na_mulmod(xp, p);
+    xp = na_mulmod(xp, xp);
+  }
+  return na_mulmod(p, c1) ^ c2;
+}
+
+// header length of the member at byte p of [0, n), 0 if malformed/truncated
+static __device__ uint64_t na_header(const uint8_t* in, uint64_t p, uint64_t n) {
+  if (n < p + 10 || in[p] != 0x1f || in[p + 1] != 0x8b || in[p + 2] != 8) return 0;
+  uint8_t flg = in[p + 3];
+  if (flg & 0xE0) return 0;
+  uint64_t o = p + 10;
+  if (flg & 4) {
+    if (o + 2 > n) return 0;
+    o += 2 + (in[o] | (in[o + 1] << 8));
+    if (o > n) return 0;
+  }
+  for (int f = 8; f <= 16; f <<= 1)
+    if (flg & f) {
+      while (o < n && in[o]) o++;
+      if (o >= n) return 0;
+      o++;
+    }
+  if (flg & 2) o += 2;
+  return o <= n ? o - p : 0;
+}
+
+__global__ void __launch_bounds__(32)
+    noalloc_kernel(const uint8_t* __restrict__ in, uint64_t n, uint8_t* __restrict__ out,
+                   uint64_t out_cap, NoAllocScratch* S) {
+  __shared__ Tables<10> T;
+  __shared__ uint32_t crc_tab[256];
+  const int lane = threadIdx.x;
+  for (uint32_t i = lane; i < 256; i += 32) {
+    uint32_t c = i;
+    for (int k = 0; k < 8; k++) c = (c >> 1) ^ (0xEDB88320u & (0u - (c & 1u)));
+    crc_tab[i] = c;
+  }
+  __syncwarp();
+  int32_t status = kOk;
+  uint64_t total = 0, pos = 0;
+  if (n < 2 || in[0] != 0x1f || in[1] != 0x8b) status = kNotGzip;
+  for (uint32_t member = 0; status == kOk; member++) {
+    if (member > 0 && (n - pos < 18 || in[pos] != 0x1f || in[pos + 1] != 0x8b)) break;
+    const uint64_t hl = na_header(in, pos, n);
+    if (hl == 0) {
+      if (member == 0) status = (n < 10 || in[2] == 8) && !(n >= 10 && (in[3] & 0xE0)) ? kTruncated : kBadHeader;
+      break;
+    }
+    ChunkDesc d{};
+    d.start_bit = d.lo_bit = d.guess_bit = d.limit_bit = (pos + hl) * 8;
+    d.stop_lo = kNoStop;
+    d.abort_bit = kNoStop;
+    d.in_end = n;
+    d.flags = kChunkMemberFirst | kChunkValid;
+    d.next = kNoChunk;
+    if (lane == 0) S->page_next = 0;  // every member starts with an empty pool
+    __syncwarp();
+    const PagePool pool{S->pages, S->owner, S->seq, &S->page_next, kNoAllocPages};
+    int32_t st = decode_chunk<10, false>(in, d, nullptr, &S->res, 0, 0, nullptr, &T, pool, lane);
+    __syncwarp();
+    const ChunkResult r = S->res;
+    if (st == kPoolExhausted) {
+      status = kNoAllocTooLarge;
+      break;
+    }
+    if (st != kOk) {
+      status = st;
+      break;
+    }
+    if (!r.final_block) {
+      status = kTruncated;
+      break;
+    }
+    const uint64_t trailer = (r.end_bit + 7) / 8;
+    if (trailer + 8 > n) {
+      status = kTruncated;
+      break;
+    }
+    if (total + r.out_len > kNoAllocMaxOut) {
+      status = kNoAllocTooLarge;
+      break;
+    }
+    if (total + r.out_len > out_cap) {
+      status = kOutTooSmall;
+      total += r.out_len;  // at least this many bytes are needed
+      break;
+    }
+    // pages were taken in order, so entry q sits at pages[q] (no markers:
+    // a member starts with the zero window)
+    for (uint64_t q = lane; q < r.out_len; q += 32) out[total + q] = (uint8_t)S->pages[q];
+    __syncwarp();
+    // CRC32: each lane one slice, combined in order by lane 0
+    const uint64_t per = (r.out_len + 31) / 32;
+    const uint64_t b0 = min((uint64_t)lane * per, r.out_len), b1 = min(b0 + per, r.out_len);
+    uint32_t c = 0xFFFFFFFFu;
+    for (uint64_t q = b0; q < b1; q++) c = (c >> 8) ^ crc_tab[(c ^ out[total + q]) & 0xFF];
+    c = ~c;
+    uint32_t crc = 0;
+    for (int l = 0; l < 32; l++) {
+      uint32_t cl = __shfl_sync(0xFFFFFFFFu, c, l);
+      uint64_t ll = min(per, r.out_len - min((uint64_t)l * per, r.out_len));
+      if (lane == 0) crc = na_crc_combine(crc, cl, ll);
+    }
+    crc = __shfl_sync(0xFFFFFFFFu, crc, 0);
+    const uint8_t* t = in + trailer;
+    const uint32_t ecrc = t[0] | (t[1] << 8) | ((uint32_t)t[2] << 16) | ((uint32_t)t[3] << 24);
+    const uint32_t eisz = t[4] | (t[5] << 8) | ((uint32_t)t[6] << 16) | ((uint32_t)t[7] << 24);
+    if ((uint32_t)r.out_len != eisz) status = kSizeMismatch;
+    else if (crc != ecrc) status = kCrcMismatch;
+    total += r.out_len;
+    pos = trailer + 8;
+    if (pos >= n) break;
+  }
+  if (lane == 0) {
+    S->status = status;
+    S->out_len = total;
+  }
+}
+
 }  // namespace gzgpu
+
+#include <mutex>
+
+#include "../../include/gzgpu.h"
+
+namespace {
+// device address of the scratch array, looked up once per device
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+void* g_noalloc_ptr[kMaxDevices] = {};
+}  // namespace
+
+extern "C" int gzgpu_decompress_device_noalloc(const void* d_in, size_t in_len, void* d_out,
+                                               size_t out_cap, size_t* out_len,
+                                               void* cuda_stream) {
+  using namespace gzgpu;
+  if (!out_len || (!d_in && in_len) || (!d_out && out_cap)) return GZGPU_INVALID_ARGUMENT;
+  *out_len = 0;
+  if (reinterpret_cast<uintptr_t>(d_in) & 3) return GZGPU_INVALID_ARGUMENT;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return GZGPU_DEVICE_ERROR;
+  void* scratch = nullptr;
+  {
+    std::lock_guard<std::mutex> g(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+      // the array's host-side name is a stand-in; the kernel needs its device address
+      if (cudaGetSymbolAddress(&g_noalloc_ptr[dev], g_noalloc_scratch) != cudaSuccess) {
+        g_noalloc_ptr[dev] = nullptr;
+        return GZGPU_DEVICE_ERROR;
+      }
+    }
+    scratch = g_noalloc_ptr[dev];
+  }
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(cuda_stream);
+  NoAllocScratch* S = reinterpret_cast<NoAllocScratch*>(scratch);
+  noalloc_kernel<<<1, 32, 0, st>>>(reinterpret_cast<const uint8_t*>(d_in), in_len,
+                                   reinterpret_cast<uint8_t*>(d_out), out_cap, S);
+  if (cudaGetLastError() != cudaSuccess) return GZGPU_DEVICE_ERROR;
+  struct {
+    int32_t status;
+    uint32_t pad;
+    uint64_t out_len;
+  } res{};
+  if (cudaMemcpyAsync(&res, scratch, sizeof(res), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess)
+    return GZGPU_DEVICE_ERROR;
+  *out_len = res.out_len;
+  if (res.status == kNotGzip) *out_len = 0;
+  return res.status;
+}

@@ -40,6 +40,7 @@ extern "C" {
 #define GZGPU_TIMEOUT 8
 #define GZGPU_TRUNCATED 9
 #define GZGPU_INVALID_ARGUMENT 12
+#define GZGPU_NOALLOC_TOO_LARGE 14 /* output beyond GZGPU_NOALLOC_MAX_OUT */
 
 /* readable bytes the device-resident entry point needs after the input */
 #define GZGPU_INPUT_PAD 1024
@@ -112,6 +113,33 @@ int gzgpu_decompress_device(gzgpu_ctx *ctx, const void *d_in, size_t in_len, voi
  * stream; returns GZGPU_OK when every stream decoded (or was not gzip). */
 int gzgpu_decompress_batch(gzgpu_ctx *ctx, const gzgpu_span *ins, size_t n, gzgpu_out *outs,
                            int *statuses);
+
+/* Decode without allocating (no counterpart in the reference).
+ *
+ * For callers that cannot call cudaMalloc: code under a pool-only allocator
+ * that must not grow, real-time paths that cannot absorb the device-wide
+ * synchronisation cudaMalloc/cudaFree may cause, and processes whose device
+ * memory is all reserved up front by another framework.  Needs no context:
+ * it runs on the current device and the caller's stream (`cuda_stream`,
+ * a cudaStream_t; NULL = the default stream), with d_in / d_out in device
+ * memory (d_in 4-byte aligned with GZGPU_INPUT_PAD readable bytes past
+ * in_len).  It calls no cudaMalloc, cudaFree or allocating library routine.
+ *
+ * Its working memory is one file-scope device array of about 8.5 MiB that
+ * every GPU loading this library holds until the process exits; so the
+ * output of one call is limited to GZGPU_NOALLOC_MAX_OUT bytes (4 MiB, all
+ * members together) and larger streams return GZGPU_NOALLOC_TOO_LARGE.  One
+ * warp decodes the members in order (no speculative chunks): made for small
+ * streams, not throughput.  The first call on a device looks the array's
+ * address up (cudaGetSymbolAddress); make that first call before any stream
+ * capture.  All calls share the array: calls whose work overlaps on the GPU
+ * (on different streams, or from different threads) race and must not be
+ * issued; calls ordered on one stream are fine.  The call waits for its
+ * stream to finish the decode and returns the status; *out_len = bytes
+ * written (or needed, on GZGPU_OUT_TOO_SMALL). */
+#define GZGPU_NOALLOC_MAX_OUT (4u << 20)
+int gzgpu_decompress_device_noalloc(const void *d_in, size_t in_len, void *d_out, size_t out_cap,
+                                    size_t *out_len, void *cuda_stream);
 
 /* Diagnostics (no reference counterpart; used by the parity tests).
  *
