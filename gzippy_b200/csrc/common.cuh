@@ -43,6 +43,7 @@ enum : int32_t {
 enum : uint32_t {
   kChunkMemberFirst = 1u,  // starts a member: zero window, never emits markers
   kChunkValid = 2u,        // has a start (member start or a finder candidate)
+  kChunkConfirmed = 4u,    // starts at a boundary the chain walk confirmed (a repair)
 };
 
 struct ChunkDesc {
@@ -59,7 +60,9 @@ struct ChunkDesc {
   uint32_t pad;
 };
 constexpr uint32_t kNoChunk = 0xFFFFFFFFu;
-constexpr int kMaxExtends = 4;  // phantom successors a chunk decodes through
+// phantom successors a speculative chunk decodes through; a chunk whose start
+// is certain (member-first or confirmed) decodes through any number of them
+constexpr int kMaxExtends = 4;
 
 struct ChunkResult {
   uint64_t end_bit;     // bit where decoding stopped

@@ -92,12 +92,19 @@ struct MemberPlan {
   uint64_t out_len;
 };
 
-// per-stream chain walk state (host)
+// chain walk state (host) of one segment of a stream: the members from one
+// planned member start up to the next planned start (`mend`), or the whole
+// stream (`last`).  Segments of a multi-member stream are walked
+// independently, so their repairs share decode passes; a segment must end
+// exactly at `mend`, else its stream is walked again as one segment.
 struct Walker {
   uint32_t stream;
-  uint32_t c0, c1;          // this stream's grid chunk ids [c0, c1)
+  uint32_t c0, c1;          // grid chunk ids of this segment [c0, c1)
   uint32_t j;               // next grid chunk to consider
   uint64_t mpos;            // next member header, relative to the stream
+  uint64_t mend = 0;        // planned start of the next segment (relative)
+  bool last = true;         // segment runs to the end of the stream
+  bool handoff_bad = false; // ended somewhere other than `mend`
   uint32_t member = 0;
   int32_t cur = -1;         // chunk being walked
   bool done = false;
@@ -332,6 +339,7 @@ int gzgpu_ctx::run(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R) 
   std::vector<ChunkDesc> hd;
   std::vector<uint32_t> hspec;
   std::vector<uint32_t> c0(ns), c1(ns);
+  std::vector<std::vector<uint32_t>> mc0(ns);  // first grid chunk of each planned member
   uint64_t cb = chunk_bytes ? chunk_bytes : pick_chunk_bytes(total_in);
   stats.chunk_bytes = cb;
   const uint64_t cbits = cb * 8;
@@ -339,6 +347,7 @@ int gzgpu_ctx::run(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R) 
     c0[s] = (uint32_t)hd.size();
     for (const Mem& m : mems[s]) {
       const uint64_t b0 = (S[s].off + m.ds) * 8, bend = (S[s].off + m.end) * 8;
+      mc0[s].push_back((uint32_t)hd.size());
       ChunkDesc d{};
       d.start_bit = d.lo_bit = d.guess_bit = b0;
       d.limit_bit = S[s].off + m.start;  // member-first: the member's header byte
@@ -414,14 +423,33 @@ int gzgpu_ctx::run(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R) 
   }
   cudaEventRecord(ev[5], st);
   // ---- 5. chain walk with repairs (host) ---------------------------------
-  std::vector<Walker> W(ns);
+  std::vector<std::vector<Walker>> SW(ns);
+  auto whole_stream = [&](uint32_t s) {
+    Walker w;
+    w.stream = s;
+    w.c0 = w.j = c0[s];
+    w.c1 = c1[s];
+    w.mpos = 0;
+    if (R[s].status != kOk || c0[s] == c1[s]) w.done = true;
+    return w;
+  };
   for (uint32_t s = 0; s < ns; s++) {
-    W[s].stream = s;
-    W[s].c0 = c0[s];
-    W[s].c1 = c1[s];
-    W[s].j = c0[s];
-    W[s].mpos = 0;
-    if (R[s].status != kOk || c0[s] == c1[s]) W[s].done = true;
+    const size_t nm = mc0[s].size();
+    if (nm <= 1 || R[s].status != kOk) {
+      SW[s].push_back(whole_stream(s));
+      continue;
+    }
+    for (size_t k = 0; k < nm; k++) {
+      Walker w;
+      w.stream = s;
+      w.c0 = w.j = mc0[s][k];
+      w.c1 = k + 1 < nm ? mc0[s][k + 1] : c1[s];
+      w.mpos = mems[s][k].start;
+      w.member = (uint32_t)k;
+      w.last = k + 1 == nm;
+      w.mend = w.last ? S[s].len : mems[s][k + 1].start;
+      SW[s].push_back(w);
+    }
   }
   auto is_valid = [&](uint32_t i) { return (hd[i].flags & kChunkValid) != 0; };
   auto is_mf = [&](uint32_t i) { return (hd[i].flags & kChunkMemberFirst) != 0; };
@@ -432,16 +460,19 @@ int gzgpu_ctx::run(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R) 
   auto fetch = [&](uint64_t abs, size_t n, uint8_t* dst) {
     cudaMemcpy(dst, cur_in + abs, n, cudaMemcpyDeviceToHost);
   };
-  auto new_chunk = [&](Walker& w, uint64_t start, uint64_t stop, uint32_t flags) {
+  // a repair starts at a confirmed boundary and stops at the start of grid
+  // chunk `next` (kNoChunk: none); like a member-first chunk it decodes on
+  // through any phantom successors it finds there
+  auto new_chunk = [&](Walker& w, uint64_t start, uint64_t stop, uint32_t flags, uint32_t next) {
     ChunkDesc d{};
     d.start_bit = d.lo_bit = d.guess_bit = d.limit_bit = start;
     if (flags & kChunkMemberFirst) d.limit_bit = S[w.stream].off + w.mpos;
     d.stop_lo = stop;
     d.abort_bit = kNoStop;
     d.in_end = S[w.stream].off + S[w.stream].len;
-    d.flags = flags | kChunkValid;
+    d.flags = flags | kChunkValid | kChunkConfirmed;
     d.stream = w.stream;
-    d.next = kNoChunk;
+    d.next = next;
     uint32_t id = (uint32_t)(hd.size() + repairs.size());
     repairs.push_back(d);
     repair_owner.push_back(w.stream);
@@ -507,7 +538,7 @@ int gzgpu_ctx::run(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R) 
             break;
           }
           w.member_order_begin = (uint32_t)w.order.size();
-          new_chunk(w, (base + w.mpos + o) * 8, kNoStop, kChunkMemberFirst);
+          new_chunk(w, (base + w.mpos + o) * 8, kNoStop, kChunkMemberFirst, kNoChunk);
           break;
         }
         w.member_order_begin = (uint32_t)w.order.size();
@@ -532,6 +563,12 @@ int gzgpu_ctx::run(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R) 
         w.member++;
         w.mpos = trailer + 8 - base;
         w.cur = -1;
+        if (!w.last) {
+          // a segment hands over exactly at the next planned member
+          w.handoff_bad = w.mpos != w.mend;
+          w.done = true;
+          break;
+        }
         continue;
       }
       // accept the chunk whose start range holds the confirmed end; discard
@@ -565,7 +602,7 @@ int gzgpu_ctx::run(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R) 
         // optimistic: the repair ends at the next candidate's start
         Walker::Checkpoint cp{w.order.size(), w.members.size(), j, w.member,
                               w.member_order_begin, w.mpos};
-        new_chunk(w, e, stop, 0);
+        new_chunk(w, e, stop, 0, j);
         uint32_t rid = (uint32_t)w.pending;
         w.pending = -1;
         w.assumed.push_back(Walker::Assumption{rid, hd[j].lo_bit, hd[j].start_bit, cp});
@@ -574,12 +611,27 @@ int gzgpu_ctx::run(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R) 
         w.j = j + 1;
         continue;
       }
-      new_chunk(w, e, stop, 0);
+      new_chunk(w, e, stop, 0, j < w.c1 ? j : kNoChunk);
       break;
     }
   };
   for (;;) {
-    for (auto& w : W) step(w);
+    for (auto& sw : SW)
+      for (auto& w : sw) step(w);
+    // a segment that ended off its planned hand-over (or failed in a way
+    // that leaves it unverified) sends its stream back to one whole walk
+    bool rewalk = false;
+    for (uint32_t s = 0; s < ns; s++) {
+      bool bad = false;
+      for (auto& w : SW[s])  // judged once its optimistic repairs are verified
+        bad |= w.handoff_bad && (w.assumed.empty() || w.assumed.back().repair < hd.size());
+      if (bad) {
+        SW[s].clear();
+        SW[s].push_back(whole_stream(s));
+        rewalk = true;
+      }
+    }
+    if (rewalk) continue;
     if (repairs.empty()) break;
     // decode all pending repairs in one pass
     const uint32_t base_id = (uint32_t)hd.size(), nr = (uint32_t)repairs.size();
@@ -619,29 +671,32 @@ int gzgpu_ctx::run(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R) 
     ms_dec_kernel += t;
     for (uint32_t k = 0; k < nr; k++)
       if (hr[base_id + k].status == kPoolExhausted) return kPoolExhausted;
-    for (Walker& w : W) {
-      if (w.pending >= 0) {
-        w.cur = w.pending;
-        w.pending = -1;
-      }
-      for (size_t a = 0; a < w.assumed.size(); a++) {
-        const Walker::Assumption& as = w.assumed[a];
-        if (as.repair < base_id) continue;  // verified in an earlier pass
-        const ChunkResult& rr = hr[as.repair];
-        if (rr.status == kOk && !rr.final_block && rr.end_bit >= as.lo && rr.end_bit <= as.hi)
-          continue;
-        // the repair ended elsewhere: resume the walk from it
-        w.order.resize(as.cp.order_size);
-        w.members.resize(as.cp.members_size);
-        w.j = as.cp.j;
-        w.member = as.cp.member;
-        w.member_order_begin = as.cp.member_order_begin;
-        w.mpos = as.cp.mpos;
-        w.cur = (int32_t)as.repair;
-        w.done = false;
-        w.status = kOk;
-        w.assumed.resize(a);
-        break;
+    for (auto& sw : SW) {
+      for (Walker& w : sw) {
+        if (w.pending >= 0) {
+          w.cur = w.pending;
+          w.pending = -1;
+        }
+        for (size_t a = 0; a < w.assumed.size(); a++) {
+          const Walker::Assumption& as = w.assumed[a];
+          if (as.repair < base_id) continue;  // verified in an earlier pass
+          const ChunkResult& rr = hr[as.repair];
+          if (rr.status == kOk && !rr.final_block && rr.end_bit >= as.lo && rr.end_bit <= as.hi)
+            continue;
+          // the repair ended elsewhere: resume the walk from it
+          w.order.resize(as.cp.order_size);
+          w.members.resize(as.cp.members_size);
+          w.j = as.cp.j;
+          w.member = as.cp.member;
+          w.member_order_begin = as.cp.member_order_begin;
+          w.mpos = as.cp.mpos;
+          w.cur = (int32_t)as.repair;
+          w.done = false;
+          w.handoff_bad = false;
+          w.status = kOk;
+          w.assumed.resize(a);
+          break;
+        }
       }
     }
     repairs.clear();
@@ -664,12 +719,12 @@ int gzgpu_ctx::run(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R) 
   const uint64_t kCrcBlock = 64 << 10;
   uint64_t last_marker_end = 0;
   for (uint32_t s = 0; s < ns; s++) {
-    Walker& w = W[s];
-    if (R[s].status == kOk) R[s].status = w.status;
+    for (Walker& w : SW[s])
+      if (R[s].status == kOk) R[s].status = w.status;
     if (R[s].status != kOk) continue;
     R[s].out_off = out_total;
     uint64_t so = 0;
-    for (MemberPlan& mp : w.members) {
+    for (Walker& w : SW[s]) for (MemberPlan& mp : w.members) {
       mp.out_len = 0;
       for (uint32_t k = mp.order_begin; k < mp.order_end; k++) mp.out_len += hr[w.order[k]].out_len;
       uint64_t moff = out_total + so;
@@ -775,7 +830,9 @@ int gzgpu_ctx::run(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R) 
     size_t mi = 0;
     for (uint32_t s = 0; s < ns; s++) {
       if (R[s].status != kOk) continue;
-      for (size_t k = 0; k < W[s].members.size(); k++, mi++)
+      size_t nm = 0;
+      for (const Walker& w : SW[s]) nm += w.members.size();
+      for (size_t k = 0; k < nm; k++, mi++)
         if (R[s].status == kOk && mst[mi] != kOk) R[s].status = mst[mi];
     }
   }

@@ -779,7 +779,8 @@ __device__ int32_t decode_chunk(const uint8_t* __restrict__ in, ChunkDesc d,
       // A block boundary past the successor's start range means that start
       // was a phantom: decode on to the start after it (the consumer's
       // re-decode from the confirmed boundary, chunk_fetcher.rs:855).
-      if (d.next == kNoChunk || extends >= kMaxExtends) break;
+      if (d.next == kNoChunk) break;
+      if (extends >= kMaxExtends && !(d.flags & (kChunkMemberFirst | kChunkConfirmed))) break;
       const ChunkDesc nx = descs[d.next];
       if ((nx.flags & kChunkMemberFirst) || bitpos <= nx.start_bit) break;
       if (nx.next == kNoChunk) {

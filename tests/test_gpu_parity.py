@@ -121,6 +121,55 @@ def test_multi_member(G, ctx):
     assert ctx.decompress(data) == np.concatenate(plains).tobytes()
 
 
+def _zlib_members(data: bytes) -> bytes:
+    out = []
+    while data[:2] == b"\x1f\x8b":
+        d = zlib.decompressobj(31)
+        out.append(d.decompress(data))
+        data = d.unused_data
+    return b"".join(out)
+
+
+def test_multi_member_segments_share_repair_passes(G):
+    """Members walk as independent segments: the repairs of all members
+    (level-1 fixed-Huffman members give the finder nothing to find) are
+    decoded in a few shared passes, not one pass per member."""
+    plains, comps = [], []
+    for k in range(48):
+        p, c = _stream(W.MARKOV if k % 2 else W.RAMPS, 1, 300_000 + 1111 * k, seed=100 + k)
+        plains.append(p)
+        comps.append(c)
+    ctx = G.Context(chunk_bytes=16 << 10)
+    assert ctx.decompress(np.concatenate(comps)) == np.concatenate(plains).tobytes()
+    s = ctx.stats()
+    assert s.n_members == 48
+    assert s.decode_passes <= 8, s.decode_passes
+    ctx.close()
+
+
+def test_multi_member_false_member_plan_rewalks(G, ctx):
+    """A member whose stored blocks carry a whole two-member gzip file: the
+    scan plans members inside it, the segment before them ends elsewhere, and
+    the stream is walked again as one segment."""
+    inner = b"".join(_gz_level(W.content(W.MARKOV, 40 + k, 90_000).tobytes(), 6)
+                     for k in range(2))
+    outer_b = _gz_level(inner, 0)
+    a = _gz_level(W.content(W.RAMPS, 43, 120_000).tobytes(), 6)
+    c = _gz_level(W.content(W.RUNS, 44, 150_000).tobytes(), 9)
+    data = a + outer_b + c
+    want = _zlib_members(data)
+    assert ctx.decompress(data) == want
+    for cb in (8 << 10, 64 << 10):
+        cx = G.Context(chunk_bytes=cb)
+        assert cx.decompress(data) == want
+        cx.close()
+
+
+def _gz_level(data: bytes, level: int) -> bytes:
+    c = zlib.compressobj(level, zlib.DEFLATED, 31)
+    return c.compress(data) + c.flush()
+
+
 def test_edge_cases(G, ctx):
     p, c = _stream(W.MARKOV, 6, 100_000, seed=2)
     cb = c.tobytes()
