@@ -22,6 +22,7 @@ own replica (weak scaling, no collective on the data path).
 from __future__ import annotations
 
 import argparse
+import ctypes
 import hashlib
 import json
 import os
@@ -80,6 +81,226 @@ def load_workload(name: str, scale: float):
     comp.tofile(path)
     json.dump(meta, open(meta_path, "w"))
     return comp, meta
+
+
+def load_batch(scale: float):
+    """The 10,000-stream batch (log-normal sizes, median 64 KiB, sigma 1.5,
+    1 KiB-64 MiB; content type uniform over the four kinds; level uniform in
+    {1, 6, 9}), packed at 16-byte aligned offsets with 1 KiB of zero pad.
+    Returns (packed, offsets, lengths, plain sizes, meta); cached on disk."""
+    from gzippy_b200 import workloads as W
+    os.makedirs(CACHE, exist_ok=True)
+    n = max(16, int(round(10000 * scale)))
+    base = os.path.join(CACHE, f"stream_batch_{n}")
+    if os.path.exists(base + ".json"):
+        meta = json.load(open(base + ".json"))
+        z = np.load(base + ".npz")
+        return z["packed"], z["offs"], z["lens"], z["sizes"], meta
+    t0 = time.time()
+    wl = W.stream_batch(streams=n, keep_plain=True)
+    lens = np.array([c.size for c in wl.compressed], np.uint64)
+    offs = np.zeros(n, np.uint64)
+    at = 0
+    for i, c in enumerate(wl.compressed):
+        offs[i] = at
+        at += (c.size + 15) & ~15
+    packed = np.zeros(at + 1024, np.uint8)
+    for o, c in zip(offs, wl.compressed):
+        packed[int(o):int(o) + c.size] = c
+    h = hashlib.sha256()
+    for p_ in wl.plain:
+        h.update(p_.tobytes())
+    sizes = np.array(wl.plain_sizes, np.uint64)
+    lv = np.array(wl.meta["levels"])
+    meta = {"name": "stream_batch", "streams": n, "plain_bytes": int(sizes.sum()),
+            "comp_bytes": int(lens.sum()), "sha256": h.hexdigest(), "gen_s": round(time.time() - t0, 2),
+            "max_stream_bytes": int(sizes.max()),
+            "levels": {str(k): int((lv == k).sum()) for k in (1, 6, 9)}}
+    np.savez(base + ".npz", packed=packed, offs=offs, lens=lens, sizes=sizes)
+    json.dump(meta, open(base + ".json", "w"))
+    return packed, offs, lens, sizes, meta
+
+
+def cpu_batch_baseline(packed, offs, lens, sizes, budget_s: float = 10.0, threads: int | None = None):
+    """The oracle's serial decoder, one stream per task, on all host threads,
+    over the first streams of the batch that fit the time budget."""
+    from concurrent.futures import ThreadPoolExecutor
+    from oracle import pyoracle as O
+    th = threads or cpus()
+
+    def one(i):
+        o, l = int(offs[i]), int(lens[i])
+        st, out = O.decompress(packed[o:o + l], cap=int(sizes[i]) + 4096)
+        assert st == O.OK and out.size == int(sizes[i])
+        return out.size
+
+    done, nbytes, t0 = 0, 0, time.perf_counter()
+    with ThreadPoolExecutor(th) as ex:
+        while done < len(offs) and time.perf_counter() - t0 < budget_s:
+            k = min(len(offs), done + 4 * th)
+            nbytes += sum(ex.map(one, range(done, k)))
+            done = k
+    dt = time.perf_counter() - t0
+    return {"value": round(nbytes / dt / 1e9, 4), "unit": "GB/s", "cores": th, "kind": "port",
+            "sample": f"first {done} of {len(offs)} streams ({nbytes >> 20} MiB out), oracle serial "
+                      f"decoder, one stream per task"}
+
+
+def bench_batch(args, rank: int, world: int, local: int):
+    """Batched path: all streams in one job per step (device-resident input and
+    output) against the plain path (one stream per call) on the same GPU."""
+    packed, offs, lens, sizes, meta = load_batch(args.scale)
+    n = len(offs)
+    config = {"workload": "stream_batch", "streams": n, "levels": meta["levels"],
+              "seed": 1237, "plain_bytes": meta["plain_bytes"], "comp_bytes": meta["comp_bytes"],
+              "max_stream_bytes": meta["max_stream_bytes"],
+              "l2": "inputs and outputs larger than the 126 MB L2; no flush",
+              "parallelism": f"replicas x{world}", "autotune": not args.no_autotune}
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        cb = cpu_batch_baseline(packed, offs, lens, sizes, budget_s=max(5.0, 4.0 * args.steps))
+        line = {"metric": METRIC, "value": cb["value"], "unit": "GB/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": None,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+                "data": "synthetic (seeded generator + zlib levels 1/6/9)", "config": config,
+                "impl": "reference", "cpu_baseline": cb,
+                "e2e": {"value": cb["value"], "unit": "GB/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+    import torch
+    torch.cuda.set_device(local)
+    import gzippy_b200 as G
+    ctx = G.Context(device=local, autotune=not args.no_autotune)
+    d_in = torch.from_numpy(packed).cuda()
+    total = meta["plain_bytes"]
+    d_out = torch.empty(total + 4096, dtype=torch.uint8, device="cuda")
+    torch.cuda.synchronize()
+
+    def step():
+        return ctx.decompress_batch_device(d_in.data_ptr(), offs, lens, d_out.data_ptr(), d_out.numel())
+
+    tune_trials = 0
+    for _ in range(args.warmup):
+        oo, ol, st = step()
+        tune_trials += ctx.stats().tune_trials
+    assert (st == 0).all() and int(ol.sum()) == total
+    byte_exact = hashlib.sha256(d_out[:total].cpu().numpy().tobytes()).hexdigest() == meta["sha256"]
+    assert byte_exact, "batched output differs from the plaintext"
+    dec_ms, launches = [], 0
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            step()
+            s = ctx.stats()
+            dec_ms.append(s.ms_decode_kernel)
+            launches += s.kernel_launches
+            st_last = s
+        e1.record()
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    value = world * args.steps * total / (ms / 1e3) / 1e9
+    clocks = clk.summary()
+
+    # ---- plain path: one stream per call, same streams, same GPU -------------
+    pctx = G.Context(device=local)
+    aoff = np.zeros(n, np.uint64)
+    at = 0
+    for i in range(n):
+        aoff[i] = at
+        at += (int(sizes[i]) + 15) & ~15
+    d_out2 = torch.empty(at + 4096, dtype=torch.uint8, device="cuda")
+    ib, ob = d_in.data_ptr(), d_out2.data_ptr()
+    for i in range(min(n, 32)):
+        pctx.decompress_device(ib + int(offs[i]), int(lens[i]), ob + int(aoff[i]), int(sizes[i]) + 16)
+    torch.cuda.synchronize()
+    p0 = torch.cuda.Event(enable_timing=True)
+    p1 = torch.cuda.Event(enable_timing=True)
+    p0.record()
+    plain_launches = 0
+    for i in range(n):
+        pctx.decompress_device(ib + int(offs[i]), int(lens[i]), ob + int(aoff[i]), int(sizes[i]) + 16)
+        plain_launches += pctx.stats().kernel_launches
+    p1.record()
+    torch.cuda.synchronize()
+    plain_ms = p0.elapsed_time(p1)
+    plain_gbs = total / (plain_ms / 1e3) / 1e9
+    host2 = d_out2.cpu().numpy()
+    h = hashlib.sha256()
+    for i in range(n):
+        h.update(host2[int(aoff[i]):int(aoff[i]) + int(sizes[i])].tobytes())
+    plain_exact = h.hexdigest() == meta["sha256"]
+    pctx.close()
+    del d_out2
+
+    # ---- e2e: the host batch call (gzgpu_decompress_batch), pinned buffers ----
+    h_in = torch.from_numpy(packed).pin_memory()
+    h_out = torch.empty(total + 16 * n + 4096, dtype=torch.uint8).pin_memory()
+    hin, hout = h_in.numpy(), h_out.numpy()
+    spans = (G.Span * n)()
+    outs = (G.Out * n)()
+    o2 = 0
+    for i in range(n):
+        spans[i] = G.Span(hin.ctypes.data + int(offs[i]), int(lens[i]))
+        outs[i] = G.Out(hout.ctypes.data + o2, int(sizes[i]) + 16, 0)
+        o2 += int(sizes[i]) + 16
+    stv = (ctypes.c_int * n)()
+    rc = ctx._lib.gzgpu_decompress_batch(ctx._h, spans, n, outs, stv)
+    assert rc == 0, rc
+    e2e_steps = args.e2e_steps or max(1, min(args.steps, 3))
+    torch.cuda.synchronize()
+    f0 = torch.cuda.Event(enable_timing=True)
+    f1 = torch.cuda.Event(enable_timing=True)
+    f0.record()
+    for _ in range(e2e_steps):
+        ctx._lib.gzgpu_decompress_batch(ctx._h, spans, n, outs, stv)
+    f1.record()
+    torch.cuda.synchronize()
+    e2e_ms = f0.elapsed_time(f1)
+    h = hashlib.sha256()
+    o2 = 0
+    for i in range(n):
+        h.update(hout[o2:o2 + int(sizes[i])].tobytes())
+        o2 += int(sizes[i]) + 16
+    e2e = {"value": round(e2e_steps * total / (e2e_ms / 1e3) / 1e9, 4), "unit": "GB/s",
+           "h2d_bytes_per_step": int(lens.sum()), "d2h_bytes_per_step": int(total),
+           "byte_exact": h.hexdigest() == meta["sha256"]}
+
+    peak, peak_kind = roofline_peak()
+    alg = meta["comp_bytes"] + total
+    kern_ms = statistics.mean(dec_ms)
+    achieved = alg / (kern_ms / 1e3) / 1e9
+    line = {"metric": METRIC, "value": round(value, 4), "unit": "GB/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+            "data": "synthetic (seeded generator + zlib levels 1/6/9)", "config": config,
+            "byte_exact": byte_exact, "e2e": e2e,
+            "plain": {"value": round(plain_gbs, 4), "unit": "GB/s", "ms": round(plain_ms, 1),
+                      "calls": n, "gpu_launches": int(plain_launches), "byte_exact": plain_exact},
+            "batched_vs_plain": round(value / plain_gbs, 2),
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 5),
+                         "peak_kind": f"{peak_kind} (MEASURED_PEAKS hbm_gbs)", "traffic": None,
+                         "kernel": "inflate_kernel", "kernel_ms": round(kern_ms, 3),
+                         "algorithmic_bytes": int(alg)},
+            "clocks": clocks, "gpu_launches": int(launches),
+            "tuned": {"chunk_bytes": int(st_last.chunk_bytes), "lut_bits": int(st_last.lut_bits),
+                      "ctas_per_sm": int(st_last.ctas_per_sm), "key": int(st_last.tune_key),
+                      "trials_in_warmup": int(tune_trials)},
+            "stages_ms": {k: round(getattr(st_last, k), 3) for k in
+                          ("ms_scan", "ms_find", "ms_decode", "ms_decode_kernel", "ms_walk",
+                           "ms_resolve", "ms_crc", "ms_total")},
+            "chunks": {"n": int(st_last.n_chunks), "rejected": int(st_last.n_rejected),
+                       "repairs": int(st_last.n_repairs), "decode_passes": int(st_last.decode_passes)}}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_batch_baseline(packed, offs, lens, sizes)
+    ctx.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
 
 
 class ClockSampler:
@@ -182,6 +403,7 @@ def main():
     ap.add_argument("--ctas-per-sm", type=int, default=0)
     ap.add_argument("--e2e-steps", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -190,6 +412,8 @@ def main():
     if args.warmup < 3:
         log("warmup raised to 3 (timing rule)")
         args.warmup = 3
+    if args.workload == "stream_batch":
+        return bench_batch(args, rank, world, local)
 
     config = {"workload": args.workload, "streams": 1, "level": 6, "seed": 1235,
               "plain_bytes": None, "comp_bytes": None,

@@ -68,10 +68,11 @@ class Stats(ctypes.Structure):
                  ("in_bytes", "out_bytes", "n_streams", "n_members", "n_chunks", "n_accepted",
                   "n_rejected", "n_repairs", "n_tail_marker_chunks", "n_pages", "decode_passes",
                   "kernel_launches", "chunk_bytes")] +
-                [("lut_bits", ctypes.c_int32), ("pad", ctypes.c_int32)])
+                [("lut_bits", ctypes.c_int32), ("ctas_per_sm", ctypes.c_int32),
+                 ("tune_key", ctypes.c_uint32), ("tune_trials", ctypes.c_uint32)])
 
     def as_dict(self) -> dict:
-        return {n: getattr(self, n) for n, _ in self._fields_ if n != "pad"}
+        return {n: getattr(self, n) for n, _ in self._fields_}
 
 
 WRITE_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t)
@@ -99,6 +100,9 @@ def lib():
             L.gzgpu_decompress_device.argtypes = [vp, vp, sz, vp, sz, ctypes.POINTER(sz)]
             L.gzgpu_decompress_to_writer.argtypes = [vp, vp, sz, WRITE_FN, vp,
                                                      ctypes.POINTER(ctypes.c_uint64)]
+            u64p = ctypes.POINTER(ctypes.c_uint64)
+            L.gzgpu_decompress_batch_device.argtypes = [vp, vp, u64p, u64p, sz, vp, sz, u64p, u64p,
+                                                        ctypes.POINTER(ctypes.c_int)]
             L.gzgpu_decompress_batch.argtypes = [vp, ctypes.POINTER(Span), sz, ctypes.POINTER(Out),
                                                  ctypes.POINTER(ctypes.c_int)]
             L.gzgpu_get_stats.argtypes = [vp, ctypes.POINTER(Stats)]
@@ -226,6 +230,27 @@ class Context:
                 raise GzippyError("Decompression", f"output needs {n.value} bytes", rc)
             _raise(rc)
         return n.value
+
+    def decompress_batch_device(self, d_in: int, in_offs, in_lens, d_out: int, out_cap: int):
+        """Many device-resident streams in one job (gzgpu_decompress_batch_device).
+        Returns (out_offs, out_lens, statuses) as numpy arrays; raises on a
+        failing stream or a too-small output."""
+        offs = np.ascontiguousarray(in_offs, dtype=np.uint64)
+        lens = np.ascontiguousarray(in_lens, dtype=np.uint64)
+        n = offs.size
+        oo = np.zeros(max(n, 1), np.uint64)
+        ol = np.zeros(max(n, 1), np.uint64)
+        st = np.zeros(max(n, 1), np.int32)
+        u64p = ctypes.POINTER(ctypes.c_uint64)
+        rc = self._lib.gzgpu_decompress_batch_device(
+            self._h, d_in, offs.ctypes.data_as(u64p), lens.ctypes.data_as(u64p), n, d_out, out_cap,
+            oo.ctypes.data_as(u64p), ol.ctypes.data_as(u64p),
+            st.ctypes.data_as(ctypes.POINTER(ctypes.c_int)))
+        if rc not in (OK, NOT_GZIP):
+            if rc == OUT_TOO_SMALL:
+                raise GzippyError("Decompression", f"output needs {int(ol[:n].sum())} bytes", rc)
+            _raise(rc)
+        return oo[:n], ol[:n], st[:n]
 
     def debug_find(self, data, ranges):
         """Finder kernel on explicit bit ranges -> list of (lo, hi) or None."""

@@ -18,6 +18,7 @@
 #include <chrono>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <new>
 #include <vector>
@@ -215,6 +216,23 @@ struct gzgpu_ctx {
   }
 
   int run(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R);
+  // run() under the autotuner when it is on
+  int job(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R);
+
+  // Autotuner: per kind of job (key), the fastest decode parameters found.
+  struct TuneCfg {
+    uint64_t chunk_bytes;
+    int lut_bits, ctas_per_sm;
+  };
+  std::map<uint32_t, TuneCfg> tune_cache;
+  bool tuning = false;     // a trial run: parameters are forced, no cache lookup
+  uint32_t last_key = 0;   // key of the last job
+  void apply(const TuneCfg& t) {
+    chunk_bytes = t.chunk_bytes;
+    lut_bits = t.lut_bits;
+    ctas_per_sm = t.ctas_per_sm;
+    setup_decode_grid();
+  }
 
   // chunk tables of the last job (diagnostics)
   std::vector<ChunkDesc> last_descs;
@@ -229,6 +247,59 @@ static uint64_t pick_chunk_bytes(uint64_t in_len) {
   if (in_len < (64ull << 20)) c = 32 << 10;
   if (in_len < (4ull << 20)) c = 16 << 10;
   return c;
+}
+
+int gzgpu_ctx::job(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R) {
+  if (!autotune) return run(S, R);
+  uint64_t total_in = 0;
+  for (const StreamSpec& s : S) total_in += s.len;
+  // jobs of a kind not tuned yet start from the defaults
+  const TuneCfg dflt{pick_chunk_bytes(total_in), 10, 3};
+  apply(dflt);
+  int rc = run(S, R);
+  if (rc != kOk || tune_cache.count(last_key)) return rc;
+  // Coordinate search, one full decode per candidate (outputs are identical,
+  // so any run's result stands): chunk size, then LUT bits, then warps/SM.
+  const uint32_t key = last_key;
+  uint32_t trials = 0;
+  auto trial = [&](const TuneCfg& t) {
+    apply(t);
+    tuning = true;
+    auto t0 = std::chrono::steady_clock::now();
+    int r = run(S, R);
+    double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    tuning = false;
+    trials++;
+    return r == kOk ? ms : 1e30;
+  };
+  TuneCfg best = dflt;
+  double best_ms = trial(best);
+  for (uint64_t cb : {16ull << 10, 32ull << 10, 64ull << 10, 128ull << 10}) {
+    if (cb == best.chunk_bytes) continue;
+    TuneCfg t = best;
+    t.chunk_bytes = cb;
+    double ms = trial(t);
+    if (ms < best_ms) best_ms = ms, best = t;
+  }
+  for (int lb : {11, 12}) {
+    TuneCfg t = best;
+    t.lut_bits = lb;
+    double ms = trial(t);
+    if (ms < best_ms) best_ms = ms, best = t;
+  }
+  {
+    TuneCfg t = best;
+    t.ctas_per_sm = 4;
+    double ms = trial(t);
+    if (ms < best_ms) best_ms = ms, best = t;
+  }
+  tune_cache[key] = best;
+  // the final decode with the chosen parameters gives the call's stats
+  apply(best);
+  stats = gzgpu_stats{};
+  rc = run(S, R);
+  stats.tune_trials = trials;
+  return rc;
 }
 
 int gzgpu_ctx::run(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R) {
@@ -279,6 +350,27 @@ int gzgpu_ctx::run(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R) 
   cudaMemcpyAsync(&n_cand, counters.p, 4, cudaMemcpyDeviceToHost, st);
   if ((rc = check(cudaStreamSynchronize(st)))) return rc;
   cudaEventRecord(ev[2], st);
+  if (autotune) {
+    // the kind of job: compressed size (log2), stream count (log4) and the
+    // share of streams whose first block is fixed-Huffman (the finder has
+    // nothing to find in fixed blocks, so such streams split less)
+    uint64_t n_ok = 0, n_fixed = 0;
+    for (uint32_t s = 0; s < ns; s++)
+      if (hinfo[s].status == kOk) {
+        n_ok++;
+        n_fixed += hinfo[s].first_btype == 1;
+      }
+    uint32_t sb = 0, nb = 0;
+    while (sb < 63 && (2ull << sb) <= total_in) sb++;
+    while (nb < 15 && (4ull << (2 * nb)) <= ns) nb++;
+    const uint32_t fb = n_ok ? (uint32_t)((n_fixed * 4 + n_ok / 2) / n_ok) : 0;
+    last_key = (sb << 8) | (nb << 4) | fb;
+    stats.tune_key = last_key;
+    if (!tuning) {
+      auto it = tune_cache.find(last_key);
+      if (it != tune_cache.end()) apply(it->second);
+    }
+  }
   n_cand = std::min(n_cand, cand_cap);
   std::vector<MemberCand> hc(n_cand);
   if (n_cand) {
@@ -342,6 +434,8 @@ int gzgpu_ctx::run(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R) 
   std::vector<std::vector<uint32_t>> mc0(ns);  // first grid chunk of each planned member
   uint64_t cb = chunk_bytes ? chunk_bytes : pick_chunk_bytes(total_in);
   stats.chunk_bytes = cb;
+  stats.lut_bits = lut_bits;
+  stats.ctas_per_sm = ring ? 0 : ctas_per_sm;
   const uint64_t cbits = cb * 8;
   for (uint32_t s = 0; s < ns; s++) {
     c0[s] = (uint32_t)hd.size();
@@ -950,7 +1044,7 @@ int gzgpu_decompress(gzgpu_ctx* c, const uint8_t* in, size_t in_len, uint8_t* ou
   c->user_out = nullptr;
   std::vector<StreamSpec> S{{0, in_len}};
   std::vector<StreamOut> R;
-  rc = c->run(S, R);
+  rc = c->job(S, R);
   if (rc != kOk) return rc;
   finish_stats(c);
   if (R[0].status != kOk) return R[0].status;
@@ -992,7 +1086,7 @@ int gzgpu_decompress_device(gzgpu_ctx* c, const void* d_in, size_t in_len, void*
   c->user_cap = out_cap;
   std::vector<StreamSpec> S{{0, in_len}};
   std::vector<StreamOut> R;
-  int rc = c->run(S, R);
+  int rc = c->job(S, R);
   c->user_out = nullptr;
   if (rc != kOk) return rc;
   finish_stats(c);
@@ -1019,7 +1113,7 @@ int gzgpu_decompress_to_writer(gzgpu_ctx* c, const uint8_t* in, size_t in_len,
   c->user_out = nullptr;
   std::vector<StreamSpec> S{{0, in_len}};
   std::vector<StreamOut> R;
-  rc = c->run(S, R);
+  rc = c->job(S, R);
   if (rc != kOk) return rc;
   finish_stats(c);
   if (R[0].status != kOk) return R[0].status;
@@ -1041,6 +1135,42 @@ int gzgpu_decompress_to_writer(gzgpu_ctx* c, const uint8_t* in, size_t in_len,
     if (written) *written = done;
   }
   return GZGPU_OK;
+}
+
+int gzgpu_decompress_batch_device(gzgpu_ctx* c, const void* d_in, const uint64_t* in_offs,
+                                  const uint64_t* in_lens, size_t n, void* d_out, size_t out_cap,
+                                  uint64_t* out_offs, uint64_t* out_lens, int* statuses) {
+  if (!c || (n && (!d_in || !in_offs || !in_lens || !out_offs || !out_lens || !statuses)))
+    return GZGPU_INVALID_ARGUMENT;
+  if ((reinterpret_cast<uintptr_t>(d_in) | reinterpret_cast<uintptr_t>(d_out)) & 15)
+    return GZGPU_INVALID_ARGUMENT;  // the kernels use 16-byte vector access
+  for (size_t i = 0; i < n; i++)
+    if (in_offs[i] & 15) return GZGPU_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> g(c->mu);
+  cudaSetDevice(c->dev);
+  reset_stats(c);
+  std::vector<StreamSpec> S(n);
+  for (size_t i = 0; i < n; i++) S[i] = StreamSpec{in_offs[i], in_lens[i]};
+  cudaEventRecord(c->ev[0], c->st);
+  c->cur_in = reinterpret_cast<const uint8_t*>(d_in);
+  c->user_out = reinterpret_cast<uint8_t*>(d_out);
+  c->user_cap = out_cap;
+  std::vector<StreamOut> R;
+  int rc = n ? c->job(S, R) : kOk;
+  c->user_out = nullptr;
+  if (rc != kOk) return rc;
+  if (n) finish_stats(c);
+  int all = GZGPU_OK;
+  uint64_t total = 0;
+  for (size_t i = 0; i < n; i++) {
+    statuses[i] = R[i].status;
+    out_offs[i] = R[i].out_off;
+    out_lens[i] = R[i].status == kOk ? R[i].out_len : 0;
+    if (R[i].status == kOk) total += R[i].out_len;
+    if (statuses[i] != GZGPU_OK && statuses[i] != GZGPU_NOT_GZIP && all == GZGPU_OK) all = statuses[i];
+  }
+  if (all == GZGPU_OK && total > out_cap) return GZGPU_OUT_TOO_SMALL;
+  return all;
 }
 
 int gzgpu_decompress_batch(gzgpu_ctx* c, const gzgpu_span* ins, size_t n, gzgpu_out* outs,
@@ -1070,7 +1200,7 @@ int gzgpu_decompress_batch(gzgpu_ctx* c, const gzgpu_span* ins, size_t n, gzgpu_
   c->cur_in = c->in.as<uint8_t>();
   c->user_out = nullptr;
   std::vector<StreamOut> R;
-  rc = c->run(S, R);
+  rc = c->job(S, R);
   if (rc != kOk) return rc;
   finish_stats(c);
   int all = GZGPU_OK;

@@ -782,17 +782,29 @@ __device__ int32_t decode_chunk(const uint8_t* __restrict__ in, ChunkDesc d,
       if (d.next == kNoChunk) break;
       if (extends >= kMaxExtends && !(d.flags & (kChunkMemberFirst | kChunkConfirmed))) break;
       const ChunkDesc nx = descs[d.next];
-      if ((nx.flags & kChunkMemberFirst) || bitpos <= nx.start_bit) break;
-      if (nx.next == kNoChunk) {
-        d.stop_lo = kNoStop;
-        d.abort_bit = kNoStop;
-      } else {
-        d.stop_lo = handover_bit(descs[nx.next]);
+      if (nx.flags & kChunkMemberFirst) break;
+      // the successor's warp may have moved its start to a later candidate
+      // (in-kernel retry) since this chunk's stop was set: read its range
+      // afresh and keep decoding while still before it.  A stale or torn
+      // read only costs a repair: the host walk checks every handover.
+      const volatile ChunkDesc* vx = descs + d.next;
+      const uint64_t nx_lo = vx->lo_bit, nx_start = vx->start_bit;
+      if (bitpos < nx_lo) {
+        d.stop_lo = nx_lo;
         if (d.abort_bit != kNoStop) d.abort_bit = d.stop_lo + slack;
+      } else {
+        if (bitpos <= nx_start) break;
+        if (nx.next == kNoChunk) {
+          d.stop_lo = kNoStop;
+          d.abort_bit = kNoStop;
+        } else {
+          d.stop_lo = handover_bit(descs[nx.next]);
+          if (d.abort_bit != kNoStop) d.abort_bit = d.stop_lo + slack;
+        }
+        d.next = nx.next;
+        extends++;
+        if (bitpos >= d.stop_lo) continue;
       }
-      d.next = nx.next;
-      extends++;
-      if (bitpos >= d.stop_lo) continue;
     }
     if (bitpos > d.abort_bit) {
       status = kOvershoot;

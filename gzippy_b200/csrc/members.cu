@@ -68,6 +68,8 @@ __global__ void stream_header_kernel(const uint8_t* __restrict__ in,
       si.header_len = (uint32_t)h;
     }
   }
+  si.first_btype = 4;
+  if (si.status == kOk && si.header_len < len) si.first_btype = (in[p + si.header_len] >> 1) & 3;
   if (len >= 4) {
     const uint8_t* t = in + p + len - 4;
     si.last_isize = t[0] | (t[1] << 8) | ((uint32_t)t[2] << 16) | ((uint32_t)t[3] << 24);

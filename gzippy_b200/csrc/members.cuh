@@ -10,7 +10,7 @@ struct StreamInfo {
   int32_t status;       // kOk, kNotGzip, kBadHeader, kTruncated
   uint32_t header_len;  // first member's header length
   uint32_t last_isize;  // last 4 bytes of the stream
-  uint32_t pad;
+  uint32_t first_btype; // BTYPE of the first block (0 stored, 1 fixed, 2 dynamic; 4 unknown)
 };
 
 struct ScanUnit {

@@ -51,7 +51,11 @@ typedef struct {
   int device;         /* CUDA device ordinal */
   size_t chunk_bytes; /* compressed bytes per speculative chunk; 0 = tuned default */
   int lut_bits;       /* litlen LUT index bits: 10, 11 or 12; 0 = tuned default */
-  int autotune;       /* 1 = choose chunk_bytes / lut_bits per job from the tuning table */
+  int autotune;       /* 1 = choose chunk_bytes, lut_bits and ctas_per_sm per job: the
+                         first job of each kind (compressed-size bucket, stream-count
+                         bucket, share of streams whose first block is fixed-Huffman)
+                         is decoded once per candidate and the fastest is kept for
+                         later jobs of that kind; overrides the three fields */
   int ring_history;   /* 1 = decode history in a shared-memory ring (3 warps/SM) instead
                          of the output pages in HBM (32 warps/SM, the default) */
   int ctas_per_sm;    /* page-history decoder: 3 (24 warps/SM, 80 registers; default) or
@@ -78,7 +82,9 @@ typedef struct {
   uint64_t n_tail_marker_chunks, n_pages, decode_passes, kernel_launches;
   uint64_t chunk_bytes;
   int32_t lut_bits;
-  int32_t pad;
+  int32_t ctas_per_sm;
+  uint32_t tune_key;    /* autotuner key of the last job (0 when autotune is off) */
+  uint32_t tune_trials; /* decodes the autotuner ran for the last call (0 = cached) */
 } gzgpu_stats;
 
 /* Create / destroy a context on cfg->device (NULL cfg = defaults). */
@@ -113,6 +119,18 @@ int gzgpu_decompress_device(gzgpu_ctx *ctx, const void *d_in, size_t in_len, voi
  * stream; returns GZGPU_OK when every stream decoded (or was not gzip). */
 int gzgpu_decompress_batch(gzgpu_ctx *ctx, const gzgpu_span *ins, size_t n, gzgpu_out *outs,
                            int *statuses);
+
+/* Device-resident form of gzgpu_decompress_batch (no reference
+ * counterpart): n streams already in device memory at d_in + in_offs[i]
+ * (offsets multiples of 16, host arrays), GZGPU_INPUT_PAD readable bytes
+ * past the end of the last stream.  All streams decode in one job and land
+ * back to back in d_out in stream order: out_offs[i] / out_lens[i] (host
+ * arrays) give each stream's range, statuses[i] its status.  Returns
+ * GZGPU_OK, the first failing stream's status, or GZGPU_OUT_TOO_SMALL when
+ * the total exceeds out_cap (then out_lens hold the sizes needed). */
+int gzgpu_decompress_batch_device(gzgpu_ctx *ctx, const void *d_in, const uint64_t *in_offs,
+                                  const uint64_t *in_lens, size_t n, void *d_out, size_t out_cap,
+                                  uint64_t *out_offs, uint64_t *out_lens, int *statuses);
 
 /* Decode without allocating (no counterpart in the reference).
  *

@@ -242,3 +242,73 @@ def test_batch_matches_individual(G, ctx):
     for i in range(61):
         assert res[i] == plains[i], i
     assert isinstance(res[61], G.GzippyError)
+
+
+def _pack16(blobs):
+    offs, at = [], 0
+    for b in blobs:
+        offs.append(at)
+        at += (len(b) + 15) & ~15
+    buf = np.zeros(at + 1024, np.uint8)
+    for o, b in zip(offs, blobs):
+        buf[o:o + len(b)] = np.frombuffer(b, np.uint8)
+    return buf, np.array(offs, np.uint64), np.array([len(b) for b in blobs], np.uint64)
+
+
+def test_batch_device_matches_individual(G, ctx):
+    """Device-resident batch: every stream's slice of the packed output equals
+    its own decode; failing and non-gzip streams report their status."""
+    import torch
+    rng = np.random.default_rng(7)
+    blobs, want = [], []
+    for k in range(60):
+        n = int(rng.integers(1, 400_000))
+        p, c = _stream(k % 4, [1, 6, 9][k % 3], n, seed=200 + k)
+        blobs.append(c.tobytes())
+        want.append(p.tobytes())
+    blobs.append(blobs[3] + blobs[4])           # two members
+    want.append(want[3] + want[4])
+    blobs.append(b"not gzip")
+    want.append(b"")
+    blobs.append(_gz_level(b"", 6))
+    want.append(b"")
+    bad = bytearray(blobs[5])
+    bad[-8] ^= 1                                 # CRC mismatch
+    blobs.append(bytes(bad))
+    want.append(None)
+    buf, offs, lens = _pack16(blobs)
+    d_in = torch.from_numpy(buf).cuda()
+    cap = sum(len(w) for w in want if w) + 4096
+    d_out = torch.empty(cap, dtype=torch.uint8, device="cuda")
+    with pytest.raises(G.GzippyError) as ei:
+        ctx.decompress_batch_device(d_in.data_ptr(), offs, lens, d_out.data_ptr(), cap)
+    assert ei.value.code == G.CRC_MISMATCH
+    good = [i for i, w in enumerate(want) if w is not None]
+    blobs_g = [blobs[i] for i in good]
+    buf, offs, lens = _pack16(blobs_g)
+    d_in = torch.from_numpy(buf).cuda()
+    oo, ol, st = ctx.decompress_batch_device(d_in.data_ptr(), offs, lens, d_out.data_ptr(), cap)
+    host = d_out.cpu().numpy()
+    for j, i in enumerate(good):
+        assert st[j] == (G.NOT_GZIP if blobs[i] == b"not gzip" else G.OK)
+        assert host[int(oo[j]):int(oo[j]) + int(ol[j])].tobytes() == want[i], i
+    with pytest.raises(G.GzippyError) as ei:
+        ctx.decompress_batch_device(d_in.data_ptr(), offs, lens, d_out.data_ptr(), 100)
+    assert ei.value.code == G.OUT_TOO_SMALL
+
+
+def test_autotune_caches_per_kind(G):
+    """The first job of a kind runs the tuning trials, the next reuses the
+    choice; every trial's output is byte-exact."""
+    p, c = _stream(W.MARKOV, 6, 3 << 20, seed=31)
+    cx = G.Context(autotune=1)
+    assert cx.decompress(c) == p.tobytes()
+    s1 = cx.stats()
+    assert s1.tune_trials >= 4 and s1.tune_key != 0
+    assert s1.chunk_bytes in (16 << 10, 32 << 10, 64 << 10, 128 << 10)
+    assert s1.lut_bits in (10, 11, 12) and s1.ctas_per_sm in (3, 4)
+    assert cx.decompress(c) == p.tobytes()
+    s2 = cx.stats()
+    assert s2.tune_trials == 0 and s2.tune_key == s1.tune_key
+    assert (s2.chunk_bytes, s2.lut_bits, s2.ctas_per_sm) == (s1.chunk_bytes, s1.lut_bits, s1.ctas_per_sm)
+    cx.close()
