@@ -266,18 +266,21 @@ class Context:
                                         va.ctypes.data)
         if rc != OK:
             _raise(rc)
-        return [(int(lo[i]), int(hi[i])) if va[i] else None for i in range(n)]
+        return [None if not va[i] else ((int(lo[i]), int(hi[i])) if va[i] == 1 else ("sync", int(lo[i])))
+                for i in range(n)]
 
     def debug_decode(self, data, chunks, cap_per):
-        """Inflate kernel on explicit chunks [(start_bit, stop_bit, member_first)].
-        Returns (results n x 6 uint64, entries n x cap_per uint16)."""
+        """Inflate kernel on explicit chunks [(start_bit, stop_bit, flags)], flags bit 0 =
+        member start, bit 1 = sync start.  Returns (results n x 7 uint64: end_bit,
+        out_len, marker_end, n_blocks, status, final_block, sync_end; entries n x
+        cap_per uint16)."""
         a = _as_u8(data)
         n = len(chunks)
         st = np.array([c[0] for c in chunks], np.uint64)
         sp = np.array([c[1] for c in chunks], np.uint64)
         mf = np.array([int(c[2]) for c in chunks], np.int32)
         ent = np.zeros((n, cap_per), np.uint16)
-        res = np.zeros((n, 6), np.uint64)
+        res = np.zeros((n, 7), np.uint64)
         rc = self._lib.gzgpu_debug_decode(self._h, a.ctypes.data, a.size, st.ctypes.data,
                                           sp.ctypes.data, mf.ctypes.data, n, ent.ctypes.data,
                                           cap_per, res.ctypes.data)
@@ -293,7 +296,7 @@ class Context:
                              ("last_page", "<u4"), ("prev_page", "<u4"), ("n_pages", "<u4"),
                              ("n_blocks", "<u4"), ("status", "<i4"), ("final_block", "<i4"),
                              ("t_start", "<u8"), ("t_end", "<u8"), ("gen", "<u4"),
-                             ("pad", "<u4")])
+                             ("sync_end", "<u4")])
 
     def last_chunks(self):
         """(descs, results) structured arrays of the last job's chunk table."""

@@ -44,7 +44,16 @@ enum : uint32_t {
   kChunkMemberFirst = 1u,  // starts a member: zero window, never emits markers
   kChunkValid = 2u,        // has a start (member start or a finder candidate)
   kChunkConfirmed = 4u,    // starts at a boundary the chain walk confirmed (a repair)
+  kChunkSync = 8u,         // starts at a symbol boundary inside a non-final fixed-Huffman
+                           // block (a sync start), not at a block header
 };
+
+// Sync starts in fixed-Huffman data: positions are walked from kSyncOffsets
+// consecutive start bits to the first symbol boundary at or past
+// from + kSyncOffsets + kSyncSpan.
+constexpr uint32_t kSyncOffsets = 64;
+constexpr uint64_t kSyncSpan = 8192;
+constexpr uint64_t kSyncFail = ~0ull;
 
 struct ChunkDesc {
   uint64_t start_bit;  // absolute bit offset in the input buffer to decode from
@@ -76,7 +85,7 @@ struct ChunkResult {
   int32_t final_block;
   uint64_t t_start, t_end;  // %globaltimer (ns) when the warp took / finished the chunk
   uint32_t gen;             // decode attempt that produced this result (page tag)
-  uint32_t pad;
+  uint32_t sync_end;        // 1: stopped at its successor's sync start (mid-block)
 };
 
 // a page's seq word: attempt (gen) in the top 8 bits, page index below

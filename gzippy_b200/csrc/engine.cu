@@ -125,6 +125,7 @@ struct Walker {
   struct Assumption {
     uint32_t repair;
     uint64_t lo, hi;  // the next chunk's acceptable start range
+    bool sync;        // the next chunk is a sync start (taken over mid-block)
     Checkpoint cp;
   };
   std::vector<Assumption> assumed;
@@ -547,6 +548,7 @@ int gzgpu_ctx::run(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R) 
   }
   auto is_valid = [&](uint32_t i) { return (hd[i].flags & kChunkValid) != 0; };
   auto is_mf = [&](uint32_t i) { return (hd[i].flags & kChunkMemberFirst) != 0; };
+  auto is_sync = [&](uint32_t i) { return (hd[i].flags & kChunkSync) != 0; };
   std::vector<ChunkDesc> repairs;
   std::vector<uint32_t> repair_owner;
   uint64_t n_rejected = 0, n_repairs = 0;
@@ -677,7 +679,10 @@ int gzgpu_ctx::run(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R) 
           j++;
           continue;
         }
-        if (!is_mf(j) && e >= hd[j].lo_bit && e <= hd[j].start_bit && hr[j].status == kOk) {
+        // a sync start is taken over only by a chunk that stopped at it
+        // mid-block, any other start only at a block boundary
+        if (!is_mf(j) && e >= hd[j].lo_bit && e <= hd[j].start_bit && hr[j].status == kOk &&
+            is_sync(j) == (r.sync_end != 0)) {
           accepted = true;
           break;
         }
@@ -696,16 +701,16 @@ int gzgpu_ctx::run(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R) 
         // optimistic: the repair ends at the next candidate's start
         Walker::Checkpoint cp{w.order.size(), w.members.size(), j, w.member,
                               w.member_order_begin, w.mpos};
-        new_chunk(w, e, stop, 0, j);
+        new_chunk(w, e, stop, r.sync_end ? kChunkSync : 0u, j);
         uint32_t rid = (uint32_t)w.pending;
         w.pending = -1;
-        w.assumed.push_back(Walker::Assumption{rid, hd[j].lo_bit, hd[j].start_bit, cp});
+        w.assumed.push_back(Walker::Assumption{rid, hd[j].lo_bit, hd[j].start_bit, is_sync(j), cp});
         w.order.push_back(rid);
         w.cur = (int32_t)j;
         w.j = j + 1;
         continue;
       }
-      new_chunk(w, e, stop, 0, j < w.c1 ? j : kNoChunk);
+      new_chunk(w, e, stop, r.sync_end ? kChunkSync : 0u, j < w.c1 ? j : kNoChunk);
       break;
     }
   };
@@ -775,7 +780,8 @@ int gzgpu_ctx::run(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R) 
           const Walker::Assumption& as = w.assumed[a];
           if (as.repair < base_id) continue;  // verified in an earlier pass
           const ChunkResult& rr = hr[as.repair];
-          if (rr.status == kOk && !rr.final_block && rr.end_bit >= as.lo && rr.end_bit <= as.hi)
+          if (rr.status == kOk && !rr.final_block && rr.end_bit >= as.lo && rr.end_bit <= as.hi &&
+              (rr.sync_end != 0) == as.sync)
             continue;
           // the repair ended elsewhere: resume the walk from it
           w.order.resize(as.cp.order_size);
@@ -1267,7 +1273,7 @@ int gzgpu_debug_find(gzgpu_ctx* c, const uint8_t* in, size_t in_len, const uint6
   }
   if ((rc = c->check(cudaStreamSynchronize(c->st)))) return rc;
   for (size_t i = 0; i < n; i++) {
-    valid[i] = (d[i].flags & kChunkValid) ? 1 : 0;
+    valid[i] = (d[i].flags & kChunkValid) ? ((d[i].flags & kChunkSync) ? 2 : 1) : 0;
     lo[i] = d[i].lo_bit;
     hi[i] = d[i].start_bit;
   }
@@ -1275,9 +1281,9 @@ int gzgpu_debug_find(gzgpu_ctx* c, const uint8_t* in, size_t in_len, const uint6
 }
 
 int gzgpu_debug_decode(gzgpu_ctx* c, const uint8_t* in, size_t in_len, const uint64_t* start,
-                       const uint64_t* stop, const int* member_first, size_t n, uint16_t* entries,
+                       const uint64_t* stop, const int* flags, size_t n, uint16_t* entries,
                        size_t cap_per, uint64_t* res) {
-  if (!c || (!in && in_len) || (n && (!start || !stop || !member_first || !res)))
+  if (!c || (!in && in_len) || (n && (!start || !stop || !flags || !res)))
     return GZGPU_INVALID_ARGUMENT;
   std::lock_guard<std::mutex> g(c->mu);
   cudaSetDevice(c->dev);
@@ -1302,9 +1308,13 @@ int gzgpu_debug_decode(gzgpu_ctx* c, const uint8_t* in, size_t in_len, const uin
     d[i].abort_bit = kNoStop;
     d[i].next = kNoChunk;
     d[i].in_end = in_len;
-    d[i].flags = kChunkValid | (member_first[i] ? kChunkMemberFirst : 0u);
+    d[i].flags = kChunkValid | ((flags[i] & 1) ? kChunkMemberFirst : 0u) |
+                 ((flags[i] & 2) ? kChunkSync : 0u);
     wl[i] = (uint32_t)i;
   }
+  // a chunk followed by a sync start may stop at it mid-block
+  for (size_t i = 0; i + 1 < n; i++)
+    if (d[i + 1].flags & kChunkSync) d[i].next = (uint32_t)(i + 1);
   uint32_t nn = (uint32_t)n;
   cudaMemsetAsync(c->counters.p, 0, 64, c->st);
   if (n) {
@@ -1328,13 +1338,14 @@ int gzgpu_debug_decode(gzgpu_ctx* c, const uint8_t* in, size_t in_len, const uin
     cudaMemcpy(sq.data(), c->seq.p, 4 * used, cudaMemcpyDeviceToHost);
   }
   for (size_t i = 0; i < n; i++) {
-    uint64_t* o = res + 6 * i;
+    uint64_t* o = res + 7 * i;
     o[0] = r[i].end_bit;
     o[1] = r[i].out_len;
     o[2] = r[i].marker_end;
     o[3] = r[i].n_blocks;
     o[4] = (uint64_t)(int64_t)r[i].status;
     o[5] = r[i].final_block;
+    o[6] = r[i].sync_end;
   }
   if (entries) {
     for (uint32_t p = 0; p < used; p++) {

@@ -68,6 +68,48 @@ __global__ void __launch_bounds__(32 * kFinderWarps)
   }
 }
 
+// Chunks the finder left without a start: look for a sync start in
+// fixed-Huffman data (finder_core.cuh fixed_walk).  One CTA of kSyncOffsets
+// threads per speculative chunk; the walk must end inside the chunk's range
+// and the input.
+__global__ void __launch_bounds__(kSyncOffsets)
+    sync_kernel(const uint8_t* __restrict__ in, ChunkDesc* descs, const uint32_t* __restrict__ spec,
+                uint32_t n_spec) {
+  __shared__ uint32_t sync_words[kSyncWords];
+  __shared__ uint64_t sync_end[kSyncOffsets];
+  if (blockIdx.x >= n_spec) return;
+  ChunkDesc& d = descs[spec[blockIdx.x]];
+  if (d.flags & kChunkValid) return;
+  const uint64_t from = d.guess_bit, to = d.limit_bit, nbytes = d.in_end;
+  const uint64_t target = from + kSyncOffsets + kSyncSpan;
+  if (target + 64 > to || target + 128 > nbytes * 8) return;
+  const uint64_t wbase = from >> 5;
+  const uint32_t* in32 = reinterpret_cast<const uint32_t*>(in);
+  for (uint32_t i = threadIdx.x; i < kSyncWords; i += blockDim.x) sync_words[i] = in32[wbase + i];
+  __syncthreads();
+  if (threadIdx.x < kSyncOffsets)
+    sync_end[threadIdx.x] = fixed_walk(sync_words, wbase, from + threadIdx.x, target);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint64_t best = kSyncFail;
+    uint32_t best_n = 1;
+    for (uint32_t i = 0; i < kSyncOffsets; i++) {
+      const uint64_t v = sync_end[i];
+      if (v == kSyncFail) continue;
+      uint32_t c = 0;
+      for (uint32_t j = 0; j < kSyncOffsets; j++) c += sync_end[j] == v;
+      if (c > best_n || (c == best_n && best != kSyncFail && v < best)) {
+        best = v;
+        best_n = c;
+      }
+    }
+    if (best != kSyncFail) {
+      d.lo_bit = d.start_bit = best;
+      d.flags |= kChunkValid | kChunkSync;
+    }
+  }
+}
+
 // stop_lo of each valid chunk = lo of the next valid chunk when that one is
 // speculative (member starts end their predecessor at BFINAL instead);
 // valid chunks are appended to the decode work list.
@@ -108,6 +150,7 @@ cudaError_t launch_finder(const uint8_t* in, ChunkDesc* descs, const uint32_t* s
                           uint32_t n_spec, cudaStream_t stream) {
   if (n_spec == 0) return cudaSuccess;
   finder_kernel<<<n_spec, 32 * kFinderWarps, 0, stream>>>(in, descs, spec, n_spec);
+  sync_kernel<<<n_spec, kSyncOffsets, 0, stream>>>(in, descs, spec, n_spec);
   return cudaGetLastError();
 }
 

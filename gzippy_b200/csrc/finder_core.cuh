@@ -285,4 +285,70 @@ static __device__ bool warp_find_first(const uint8_t* __restrict__ in, uint64_t 
   return have;
 }
 
+// ---------------------------------------------------------------------------
+// Sync starts in fixed-Huffman data (no counterpart in the reference, whose
+// finder has no fixed-Huffman candidates: a fixed block has no header to
+// test).  A walk decodes only positions with the fixed code of RFC 1951
+// 3.2.6: a literal/length code, a length's extra bits, the 5-bit distance
+// code and its extra bits; EOB must be followed by another fixed-block
+// header.  Walks from a true symbol boundary never fail and all reach the
+// same first boundary at or past the target; walks from a wrong bit fail
+// (codes 286-287, distance codes 30-31, a non-fixed header) or fall into
+// step with the true boundaries.  The search walks kSyncOffsets start bits
+// and takes the end position most walks agree on (at least two; ties go to
+// the lower position).  Whether that position really is a boundary is
+// decided by the predecessor chunk, which hands over only on reaching it as
+// a symbol start inside a non-final fixed block.
+// ---------------------------------------------------------------------------
+static __constant__ uint8_t f_len_extra[29] = {0, 0, 0, 0, 0, 0, 0, 0, 1, 1, 1, 1, 2, 2, 2,
+                                               2, 3, 3, 3, 3, 4, 4, 4, 4, 5, 5, 5, 5, 0};
+static __constant__ uint8_t f_dist_extra[30] = {0, 0, 0, 0, 1, 1, 2, 2, 3, 3, 4, 4, 5, 5, 6,
+                                                6, 7, 7, 8, 8, 9, 9, 10, 10, 11, 11, 12, 12, 13, 13};
+
+// k <= 25 bits at absolute bit p from staged words sw (sw[0] = input word wbase)
+static __device__ __forceinline__ uint32_t staged_bits(const uint32_t* sw, uint64_t wbase,
+                                                       uint64_t p, int k) {
+  const uint32_t i = (uint32_t)((p >> 5) - wbase), sh = (uint32_t)(p & 31);
+  const uint64_t v = (((uint64_t)sw[i + 1] << 32) | sw[i]) >> sh;
+  return (uint32_t)v & ((1u << k) - 1);
+}
+
+// first symbol boundary >= target of the fixed-code walk from p, or kSyncFail
+static __device__ uint64_t fixed_walk(const uint32_t* sw, uint64_t wbase, uint64_t p,
+                                      uint64_t target) {
+  while (p < target) {
+    const uint32_t x = staged_bits(sw, wbase, p, 9);
+    const uint32_t c7 = __brev(x & 127u) >> 25, c8 = __brev(x & 255u) >> 24;
+    uint32_t sym;
+    if (c7 <= 0x17) {
+      sym = 256 + c7;
+      p += 7;
+    } else if (c8 <= 0xBF) {
+      sym = c8 - 0x30;
+      p += 8;
+    } else if (c8 <= 0xC7) {
+      sym = 280 + (c8 - 0xC0);
+      p += 8;
+    } else {
+      sym = 144 + ((__brev(x) >> 23) - 0x190);
+      p += 9;
+    }
+    if (sym < 256) continue;
+    if (sym == 256) {
+      if ((staged_bits(sw, wbase, p, 3) >> 1) != 1) return kSyncFail;
+      p += 3;
+      continue;
+    }
+    if (sym > 285) return kSyncFail;
+    p += f_len_extra[sym - 257];
+    const uint32_t dc = __brev(staged_bits(sw, wbase, p, 5)) >> 27;
+    if (dc >= 30) return kSyncFail;
+    p += 5 + f_dist_extra[dc];
+  }
+  return p;
+}
+
+// words a sync search from `from` stages: [from >> 5, (target + 96) >> 5] + 1
+constexpr uint32_t kSyncWords = (uint32_t)((kSyncOffsets + kSyncSpan + 96 + 64) / 32) + 2;
+
 }  // namespace gzgpu

@@ -535,11 +535,22 @@ template <int LB>
 __device__ int32_t huff_block_parallel(BitReader& br, const Tables<LB>* T, PageHist& ph,
                                        const PagePool& pool, uint32_t cid, uint32_t gen,
                                        uint64_t& o, uint64_t& guard, uint64_t& marker_end,
-                                       bool zero_window, uint64_t trunc_words, int lane) {
+                                       bool zero_window, uint64_t trunc_words,
+                                       uint64_t sync_target, bool& synced, int lane) {
   constexpr uint32_t LMASK = (1u << LB) - 1, DMASK = (1u << kDistBits) - 1;
   uint64_t pos = br.pos();
   int32_t status = kOk;
   for (;;) {
+    // the successor's sync start: stop exactly there if it is a symbol
+    // start of this block; rt = its offset in this step (>= 32: not here)
+    uint32_t rt = 1000;
+    if (sync_target != kNoStop && sync_target >= pos) {
+      if (sync_target == pos) {
+        synced = true;
+        break;
+      }
+      if (sync_target - pos < 32) rt = (uint32_t)(sync_target - pos);
+    }
     if (o >= guard) {
       ph.advance(o);
       if (!ph.ensure(pool, cid, gen, o + kStepMaxOut, lane)) {
@@ -609,6 +620,7 @@ __device__ int32_t huff_block_parallel(BitReader& br, const Tables<LB>* T, PageH
     // (chain positions stay below 32 + 48)
     const uint32_t kind0 = (info >> 6) & 3;
     uint32_t nxt = ((info & 0x100) || kind0 >= kKindEob) ? 128u + lane : lane + (info & 63);
+    if (nxt == rt) nxt = 96;  // the walk ends at the sync start
     // walk the chain of symbols that start in bits [0, 32)
     uint32_t path = 0, p = 0;
     bool eob = false;
@@ -646,12 +658,15 @@ __device__ int32_t huff_block_parallel(BitReader& br, const Tables<LB>* T, PageH
           eob = true;
           break;
         }
+        if (p == rt) p = 96;
         continue;
       }
       path |= 1u << p;
       p = __shfl_sync(0xFFFFFFFFu, nxt, p & 31);
     }
     if (status != kOk) break;
+    const bool at_sync = p == 96;
+    if (at_sync) p = rt;
     // output offsets: exclusive prefix sum of output lengths along the chain
     const bool on = (path >> lane) & 1;
     const uint32_t kind = (info >> 6) & 3;
@@ -712,6 +727,10 @@ __device__ int32_t huff_block_parallel(BitReader& br, const Tables<LB>* T, PageH
     __syncwarp();
     o += step_out;
     pos += p;
+    if (at_sync) {
+      synced = true;
+      break;
+    }
     if (eob) break;
   }
   br.seek(pos, lane);
@@ -773,6 +792,9 @@ __device__ int32_t decode_chunk(const uint8_t* __restrict__ in, ChunkDesc d,
 
   int extends = 0;
   const uint64_t slack = d.abort_bit != kNoStop ? d.abort_bit - d.stop_lo : 0;
+  // a sync start begins inside a non-final fixed-Huffman block (no header)
+  bool in_fixed_block = (d.flags & kChunkSync) != 0;
+  bool synced = false;
   for (;;) {
     uint64_t bitpos = br.pos();
     if (bitpos >= d.stop_lo) {
@@ -793,7 +815,10 @@ __device__ int32_t decode_chunk(const uint8_t* __restrict__ in, ChunkDesc d,
         d.stop_lo = nx_lo;
         if (d.abort_bit != kNoStop) d.abort_bit = d.stop_lo + slack;
       } else {
-        if (bitpos <= nx_start) break;
+        // a sync start is taken over only mid-block, at its exact symbol
+        // start (huff_block_parallel); a block boundary at or past it
+        // means this chunk went by it
+        if (!(nx.flags & kChunkSync) && bitpos <= nx_start) break;
         if (nx.next == kNoChunk) {
           d.stop_lo = kNoStop;
           d.abort_bit = kNoStop;
@@ -814,10 +839,18 @@ __device__ int32_t decode_chunk(const uint8_t* __restrict__ in, ChunkDesc d,
       status = kTruncated;
       break;
     }
-    br.refill(lane);
-    uint32_t hdr = (uint32_t)br.bb & 7;
-    br.consume(3);
-    uint32_t bfinal = hdr & 1, btype = hdr >> 1;
+    uint32_t bfinal, btype;
+    if (in_fixed_block) {
+      in_fixed_block = false;
+      bfinal = 0;
+      btype = 1;
+    } else {
+      br.refill(lane);
+      const uint32_t hdr = (uint32_t)br.bb & 7;
+      br.consume(3);
+      bfinal = hdr & 1;
+      btype = hdr >> 1;
+    }
     if (btype == 0) {
       // stored block: byte-align, LEN/NLEN, raw copy
       br.consume(br.bc & 7);
@@ -864,9 +897,16 @@ __device__ int32_t decode_chunk(const uint8_t* __restrict__ in, ChunkDesc d,
       status = read_tables<LB>(br, btype, T, trunc_words, lane);
       if (status != kOk) break;
       if (!kRing) {
+        // the successor's sync start can be taken over inside a non-final
+        // fixed block only (the state a sync start assumes)
+        uint64_t sync_target = kNoStop;
+        if (btype == 1 && !bfinal && d.next != kNoChunk) {
+          const ChunkDesc& nx = descs[d.next];
+          if (nx.flags & kChunkSync) sync_target = nx.start_bit;
+        }
         status = huff_block_parallel<LB>(br, T, ph, pool, cid, gen, o, guard, marker_end,
-                                         zero_window, trunc_words, lane);
-        if (status != kOk) break;
+                                         zero_window, trunc_words, sync_target, synced, lane);
+        if (status != kOk || synced) break;
         n_blocks++;
         if (bfinal) {
           final_block = 1;
@@ -1021,6 +1061,7 @@ __device__ int32_t decode_chunk(const uint8_t* __restrict__ in, ChunkDesc d,
     res->status = status;
     res->final_block = final_block;
     res->gen = gen;
+    res->sync_end = synced ? 1u : 0u;
   }
   __syncwarp();
   return status;
@@ -1043,7 +1084,8 @@ __device__ __forceinline__ void work_loop(const uint8_t* __restrict__ in, ChunkD
     ChunkDesc d = descs[cid];
     uint64_t t0 = 0;
     if (lane == 0) asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
-    const bool speculative = !(d.flags & kChunkMemberFirst) && d.limit_bit > d.lo_bit;
+    const bool speculative =
+        !(d.flags & (kChunkMemberFirst | kChunkSync)) && d.limit_bit > d.lo_bit;
     for (uint32_t gen = 0;; gen++) {
       int32_t st = decode_chunk<LB, kRing>(in, d, descs, &results[cid], cid, gen, ring, T, pool,
                                            lane);

@@ -163,19 +163,22 @@ int gzgpu_decompress_device_noalloc(const void *d_in, size_t in_len, void *d_out
  *
  * gzgpu_debug_find: run the block-finder kernel on `in` for n ranges
  * [from[i], to[i]) (bit offsets); lo/hi = first candidate's (bit_offset,
- * seek_bit), valid[i] = 0 when the range holds none.  Mirrors
- * DeflateBlockValidator::find_first_candidate
+ * seek_bit), valid[i] = 0 when the range holds none, 1 for a block header,
+ * 2 for a sync start in fixed-Huffman data (lo = hi = its bit; no
+ * reference counterpart).  Mirrors DeflateBlockValidator::find_first_candidate
  * (src/decompress/parallel/blockfinder_validation.rs:319).
  *
  * gzgpu_debug_decode: run the inflate kernel on n explicit chunks (start
- * bit, stop bit, member_first = zero window instead of markers) and copy
- * each chunk's u16 entries to entries + i*cap_per.  res[6*i..] = end_bit,
- * out_len, marker_end, n_blocks, status, final_block.  Mirrors
- * decode_chunk (src/decompress/parallel/chunk_decode.rs:225). */
+ * bit, stop bit, flags[i]: bit 0 = member start (zero window instead of
+ * markers), bit 1 = sync start) and copy each chunk's u16 entries to
+ * entries + i*cap_per.  A chunk followed by sync starts may stop at them
+ * mid-block.  res[7*i..] = end_bit, out_len, marker_end, n_blocks, status,
+ * final_block, sync_end.  Mirrors decode_chunk
+ * (src/decompress/parallel/chunk_decode.rs:225). */
 int gzgpu_debug_find(gzgpu_ctx *ctx, const uint8_t *in, size_t in_len, const uint64_t *from,
                      const uint64_t *to, size_t n, uint64_t *lo, uint64_t *hi, int *valid);
 int gzgpu_debug_decode(gzgpu_ctx *ctx, const uint8_t *in, size_t in_len, const uint64_t *start,
-                       const uint64_t *stop, const int *member_first, size_t n, uint16_t *entries,
+                       const uint64_t *stop, const int *flags, size_t n, uint16_t *entries,
                        size_t cap_per, uint64_t *res);
 
 /* gzgpu_debug_last_chunks: the chunk table of the last job.  descs holds
@@ -183,7 +186,7 @@ int gzgpu_debug_decode(gzgpu_ctx *ctx, const uint8_t *in, size_t in_len, const u
  * in_end, abort_bit as u64; flags, stream, next, pad as u32); results n records of 72
  * bytes (end_bit, out_len, marker_end as u64; last_page, prev_page, n_pages,
  * n_blocks as u32; status, final_block as i32; t_start, t_end as u64 device
- * nanoseconds; gen as u32 + 4 pad bytes: 72 bytes).  *n = records available (copies min(cap, *n)). */
+ * nanoseconds; gen, sync_end as u32: 72 bytes).  *n = records available (copies min(cap, *n)). */
 int gzgpu_debug_last_chunks(gzgpu_ctx *ctx, void *descs, void *results, size_t cap, size_t *n);
 
 /* Statistics of the last call. */

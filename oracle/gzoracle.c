@@ -359,24 +359,51 @@ int orc_dynamic_lengths(const uint8_t *data, size_t n, uint64_t bit, uint8_t *le
 /* boundary >= stop_lo, as in chunk_decode.rs decode_chunk :225 with          */
 /* stop_hint; the BFINAL block always ends the chunk.                          */
 /* ------------------------------------------------------------------------ */
-int orc_inflate_chunk(const uint8_t *data, size_t n, uint64_t start_bit, uint64_t stop_lo,
-                      int window_mode, const uint8_t *window, size_t wlen, uint16_t *out,
-                      size_t cap, orc_chunk_result *res) {
+/* Core of orc_inflate_chunk, with the two modes of the device decoder's
+ * sync starts (no counterpart in the reference):
+ *   ORC_START_FIXED: start_bit is a symbol start inside a non-final
+ *     fixed-Huffman block (no header is read for the first block);
+ *   sync targets: the chunk's successors are sync starts t[0] < t[1] < ...;
+ *     while decoding a non-final fixed block the chunk stops at the symbol
+ *     start == t[k] of its current successor k (*sync_end = 1).  At a block
+ *     boundary at or past t[k] it has gone by successor k and moves on to
+ *     k + 1; past the last one it stops only at the final block.
+ * Without targets the stop rule is the first block boundary >= stop_lo. */
+static int inflate_core(const uint8_t *data, size_t n, uint64_t start_bit, uint64_t stop_lo,
+                        int flags, const uint64_t *targets, size_t n_targets, int window_mode,
+                        const uint8_t *window, size_t wlen, uint16_t *out, size_t cap,
+                        orc_chunk_result *res, uint32_t *sync_end) {
   pthread_once(&fixed_once, fixed_init);
   br_t b = {data, n, start_bit};
   uint64_t o = 0, marker_end = 0;
   uint32_t nblocks = 0, nbt[3] = {0, 0, 0};
-  int final_block = 0, st = ORC_OK;
+  int final_block = 0, st = ORC_OK, synced = 0;
+  int in_fixed = (flags & ORC_START_FIXED) != 0;
+  size_t cur = 0;
   htab_t *lit = NULL, *dist = NULL;
   htab_t *dyn = (htab_t *)malloc(2 * sizeof(htab_t));
   if (wlen > WIN) {
     window += wlen - WIN;
     wlen = WIN;
   }
+  if (n_targets) stop_lo = targets[0];
   for (;;) {
+    if (n_targets) {
+      while (cur < n_targets && b.pos >= targets[cur]) cur++;
+      stop_lo = cur < n_targets ? targets[cur] : (uint64_t)-1;
+    }
     if (b.pos >= stop_lo) break;
-    uint32_t hdr = (uint32_t)br_read(&b, 3);
-    int bfinal = hdr & 1, btype = hdr >> 1;
+    int bfinal, btype;
+    if (in_fixed) {
+      in_fixed = 0;
+      bfinal = 0;
+      btype = 1;
+    } else {
+      uint32_t hdr = (uint32_t)br_read(&b, 3);
+      bfinal = hdr & 1;
+      btype = hdr >> 1;
+    }
+    const uint64_t watch = (btype == 1 && !bfinal && cur < n_targets) ? targets[cur] : (uint64_t)-1;
     if (br_over(&b)) { st = ORC_TRUNCATED; break; }
     if (btype == 0) {
       b.pos = (b.pos + 7) & ~7ull;
@@ -400,6 +427,7 @@ int orc_inflate_chunk(const uint8_t *data, size_t n, uint64_t start_bit, uint64_
         if (e) { st = e; break; }
       }
       for (;;) {
+        if (b.pos == watch) { synced = 1; break; }
         if (br_over(&b)) { st = ORC_TRUNCATED; break; }
         int sym = htab_decode(lit, &b);
         if (sym < 0) { st = ORC_BAD_DEFLATE; break; }
@@ -435,7 +463,7 @@ int orc_inflate_chunk(const uint8_t *data, size_t n, uint64_t start_bit, uint64_
           if (v >= 256) marker_end = o + 1;
         }
       }
-      if (st) break;
+      if (st || synced) break;
       if (br_over(&b)) { st = ORC_TRUNCATED; break; }
     } else {
       st = ORC_BAD_DEFLATE;
@@ -449,6 +477,7 @@ int orc_inflate_chunk(const uint8_t *data, size_t n, uint64_t start_bit, uint64_
     }
   }
   free(dyn);
+  if (sync_end) *sync_end = (uint32_t)synced;
   res->end_bit = b.pos;
   res->out_len = o;
   res->marker_end = marker_end;
@@ -459,6 +488,84 @@ int orc_inflate_chunk(const uint8_t *data, size_t n, uint64_t start_bit, uint64_
   res->final_block = final_block;
   res->status = st;
   return st;
+}
+
+int orc_inflate_chunk(const uint8_t *data, size_t n, uint64_t start_bit, uint64_t stop_lo,
+                      int window_mode, const uint8_t *window, size_t wlen, uint16_t *out,
+                      size_t cap, orc_chunk_result *res) {
+  return inflate_core(data, n, start_bit, stop_lo, 0, NULL, 0, window_mode, window, wlen, out,
+                      cap, res, NULL);
+}
+
+int orc_inflate_chunk_ex(const uint8_t *data, size_t n, uint64_t start_bit, uint64_t stop_lo,
+                         int flags, const uint64_t *sync_targets, size_t n_targets,
+                         uint16_t *out, size_t cap, orc_chunk_result *res, uint32_t *sync_end) {
+  return inflate_core(data, n, start_bit, stop_lo, flags, sync_targets, n_targets,
+                      (flags & ORC_ZERO_WINDOW) ? ORC_WIN_BYTES : ORC_WIN_MARKERS, NULL, 0, out,
+                      cap, res, sync_end);
+}
+
+/* ------------------------------------------------------------------------ */
+/* Sync starts in fixed-Huffman data (no counterpart in the reference; the  */
+/* device finder's fixed_walk / sync search restated for the parity tests). */
+/* ------------------------------------------------------------------------ */
+static const uint8_t FW_LEN_EXTRA[29] = {0, 0, 0, 0, 0, 0, 0, 0, 1, 1, 1, 1, 2, 2, 2,
+                                         2, 3, 3, 3, 3, 4, 4, 4, 4, 5, 5, 5, 5, 0};
+static const uint8_t FW_DIST_EXTRA[30] = {0, 0, 0, 0, 1, 1, 2, 2, 3, 3, 4, 4, 5, 5, 6,
+                                          6, 7, 7, 8, 8, 9, 9, 10, 10, 11, 11, 12, 12, 13, 13};
+#define SYNC_FAIL ((uint64_t)-1)
+
+static uint64_t fixed_walk(const uint8_t *d, size_t n, uint64_t p, uint64_t target) {
+  while (p < target) {
+    uint32_t x = (uint32_t)bits_at(d, n, p, 9);
+    uint32_t c7 = rev_bits(x & 127u, 7), c8 = rev_bits(x & 255u, 8), sym;
+    if (c7 <= 0x17) {
+      sym = 256 + c7;
+      p += 7;
+    } else if (c8 <= 0xBF) {
+      sym = c8 - 0x30;
+      p += 8;
+    } else if (c8 <= 0xC7) {
+      sym = 280 + (c8 - 0xC0);
+      p += 8;
+    } else {
+      sym = 144 + (rev_bits(x, 9) - 0x190);
+      p += 9;
+    }
+    if (sym < 256) continue;
+    if (sym == 256) {
+      if ((bits_at(d, n, p, 3) >> 1) != 1) return SYNC_FAIL;
+      p += 3;
+      continue;
+    }
+    if (sym > 285) return SYNC_FAIL;
+    p += FW_LEN_EXTRA[sym - 257];
+    uint32_t dc = rev_bits((uint32_t)bits_at(d, n, p, 5), 5);
+    if (dc >= 30) return SYNC_FAIL;
+    p += 5 + FW_DIST_EXTRA[dc];
+  }
+  return p;
+}
+
+int orc_fixed_sync_find(const uint8_t *data, size_t n, uint64_t from, uint64_t to, uint64_t *bit) {
+  const uint64_t target = from + ORC_SYNC_OFFSETS + ORC_SYNC_SPAN;
+  if (target + 64 > to || target + 128 > (uint64_t)n * 8) return 0;
+  uint64_t e[ORC_SYNC_OFFSETS];
+  for (int i = 0; i < ORC_SYNC_OFFSETS; i++) e[i] = fixed_walk(data, n, from + i, target);
+  uint64_t best = SYNC_FAIL;
+  int best_n = 1;
+  for (int i = 0; i < ORC_SYNC_OFFSETS; i++) {
+    if (e[i] == SYNC_FAIL) continue;
+    int c = 0;
+    for (int j = 0; j < ORC_SYNC_OFFSETS; j++) c += e[j] == e[i];
+    if (c > best_n || (c == best_n && best != SYNC_FAIL && e[i] < best)) {
+      best = e[i];
+      best_n = c;
+    }
+  }
+  if (best == SYNC_FAIL) return 0;
+  *bit = best;
+  return 1;
 }
 
 void orc_resolve_markers(const uint16_t *in, size_t n, const uint8_t *window32k, uint8_t *out) {

@@ -33,6 +33,14 @@ enum {
   ORC_TRUNCATED = 9,
 };
 
+/* flags of orc_inflate_chunk_ex */
+enum {
+  ORC_START_FIXED = 1, /* start inside a non-final fixed-Huffman block (a sync start) */
+  ORC_ZERO_WINDOW = 2, /* back-references before the chunk read zeros (member start) */
+};
+#define ORC_SYNC_OFFSETS 64
+#define ORC_SYNC_SPAN 8192
+
 /* window modes for orc_inflate_chunk */
 enum {
   ORC_WIN_MARKERS = 0, /* window unknown: back-refs before the chunk emit u16 markers */
@@ -89,6 +97,14 @@ int orc_inflate_chunk(const uint8_t *data, size_t n, uint64_t start_bit, uint64_
                       size_t cap, orc_chunk_result *res);
 
 /* code lengths of the dynamic block header at `bit` (litlen then dist) */
+/* orc_inflate_chunk with sync-start modes (no reference counterpart; the
+ * device decoder's sync starts in fixed-Huffman data): see gzoracle.c
+ * inflate_core.  *sync_end = 1 when the chunk stopped at a sync target. */
+int orc_inflate_chunk_ex(const uint8_t *data, size_t n, uint64_t start_bit, uint64_t stop_lo,
+                         int flags, const uint64_t *sync_targets, size_t n_targets,
+                         uint16_t *out, size_t cap, orc_chunk_result *res, uint32_t *sync_end);
+/* Sync start in fixed-Huffman data for the range [from, to): 1 and *bit, or 0. */
+int orc_fixed_sync_find(const uint8_t *data, size_t n, uint64_t from, uint64_t to, uint64_t *bit);
 int orc_dynamic_lengths(const uint8_t *data, size_t n, uint64_t bit, uint8_t *lens, int *nlen,
                         int *ndist);
 

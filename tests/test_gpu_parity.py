@@ -312,3 +312,76 @@ def test_autotune_caches_per_kind(G):
     assert s2.tune_trials == 0 and s2.tune_key == s1.tune_key
     assert (s2.chunk_bytes, s2.lut_bits, s2.ctas_per_sm) == (s1.chunk_bytes, s1.lut_bits, s1.ctas_per_sm)
     cx.close()
+
+
+def _level1(ctype, n, seed):
+    p = W.content(ctype, seed, n)
+    return p, W.gzip_member(p, 1)   # level 1 = fixed-Huffman blocks (stored for random bytes)
+
+
+def test_sync_find_matches_oracle(ctx):
+    """Partitions without a block header get the oracle's sync start in
+    fixed-Huffman data (or none)."""
+    for ctype, seed in ((W.MARKOV, 41), (W.RUNS, 42), (W.RAMPS, 43)):
+        p, c = _level1(ctype, 3 << 20, seed)
+        nbits = c.size * 8
+        ranges = [(f, min(f + 40 * 1024 * 8, nbits)) for f in range(200, nbits, 37 * 1024 * 8 + 5)]
+        got = ctx.debug_find(c, ranges)
+        n_sync = 0
+        for (f, t), g in zip(ranges, got):
+            first, seek = O.find_blocks(c, f, t, cap=1 << 18)
+            if first.size:
+                exp = (int(first[0]), int(seek[0]))
+            else:
+                b = O.fixed_sync_find(c, f, t)
+                exp = ("sync", b) if b is not None else None
+            n_sync += exp is not None and exp[0] == "sync"
+            assert g == exp, (ctype, f, t, g, exp)
+        if ctype != W.RAMPS:
+            assert n_sync > len(ranges) // 2
+
+
+def test_sync_chunks_match_oracle(G, ctx):
+    """Chunks that start at sync starts (mid-block, fixed table) and chunks
+    that stop at them: entries, end bits and sync_end equal the oracle's,
+    including a bogus sync start that the predecessor goes by."""
+    p, c = _level1(W.MARKOV, 2 << 20, 44)
+    _, hl = O.gzip_header_len(c)
+    nbits = c.size * 8
+    step = 40 * 1024 * 8
+    syncs = [O.fixed_sync_find(c, g, g + step) for g in range(hl * 8 + step, nbits - step, step)]
+    syncs = [b for b in syncs if b is not None]
+    assert len(syncs) >= 4
+    starts = syncs[:2] + [syncs[2] + 1] + syncs[2:]          # a bogus one before a true one
+    chunks = [(hl * 8, starts[0], 1)] + [
+        (s, starts[k + 1] if k + 1 < len(starts) else 2**64 - 1, 2) for k, s in enumerate(starts)]
+    cap = 4 << 20
+    res, ent = ctx.debug_decode(c, chunks, cap)
+    n_synced = 0
+    for i, (s, stop, fl) in enumerate(chunks):
+        targets = starts[i:i + 5]                             # successors: all sync starts
+        st, r, e, se = O.inflate_chunk_ex(c, s, stop, flags=(O.START_FIXED if fl & 2 else O.ZERO_WINDOW),
+                                          sync_targets=targets, cap=cap)
+        assert int(res[i, 4]) == st, i
+        if st != O.OK:
+            continue
+        assert int(res[i, 0]) == r.end_bit and int(res[i, 1]) == r.out_len, i
+        assert int(res[i, 2]) == r.marker_end and int(res[i, 5]) == r.final_block, i
+        assert int(res[i, 3]) == r.n_blocks and int(res[i, 6]) == se, i
+        assert np.array_equal(ent[i, :r.out_len], e), i
+        n_synced += se
+    assert n_synced >= 3
+
+
+def test_level1_fixed_streams_split(G):
+    """Fixed-Huffman members decode in many accepted chunks, byte-exact."""
+    for ctype in (W.MARKOV, W.RUNS):
+        p, c = _level1(ctype, 6 << 20, 45 + ctype)
+        cx = G.Context(chunk_bytes=32 << 10)
+        assert cx.decompress(c) == p.tobytes()
+        s = cx.stats()
+        d, r = cx.last_chunks()
+        assert s.n_accepted >= 8, (ctype, s.n_accepted)
+        assert int(((d["flags"] & 8) != 0).sum()) >= 4
+        assert int(r["sync_end"].sum()) >= 4
+        cx.close()
