@@ -240,6 +240,9 @@ struct gzgpu_ctx {
   std::vector<ChunkResult> last_results;
 };
 
+// shortest partition of a high-ratio member (8 KiB of compressed input)
+constexpr uint64_t kMinPartitionBits = 8ull << 13;
+
 static uint64_t pick_chunk_bytes(uint64_t in_len) {
   // about two chunks per decoding warp on large inputs; smaller chunks for
   // small inputs so the warps still fill (measured on the 1 GiB mixed stream:
@@ -451,10 +454,18 @@ int gzgpu_ctx::run(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R) 
       d.flags = kChunkMemberFirst | kChunkValid;
       d.stream = s;
       hd.push_back(d);
-      for (uint64_t g = b0 + cbits; g < bend; g += cbits) {
+      // members that expand a lot (ISIZE over compressed size) get shorter
+      // partitions, so chunks carry similar output (about 2 x chunk_bytes)
+      uint64_t mbits = cbits;
+      const uint64_t clen = m.end > m.ds ? m.end - m.ds : 0;
+      if (clen && (uint64_t)m.isize > 2 * clen) {
+        mbits = (uint64_t)((double)cbits * 2.0 * (double)clen / (double)m.isize) & ~63ull;
+        mbits = std::max<uint64_t>(mbits, std::min<uint64_t>(cbits, kMinPartitionBits));
+      }
+      for (uint64_t g = b0 + mbits; g < bend; g += mbits) {
         ChunkDesc x{};
         x.start_bit = x.lo_bit = x.guess_bit = g;
-        x.limit_bit = std::min(g + cbits, bend);
+        x.limit_bit = std::min(g + mbits, bend);
         x.stop_lo = kNoStop;
         x.in_end = d.in_end;
         x.flags = 0;

@@ -774,8 +774,13 @@ __device__ int32_t decode_chunk(const uint8_t* __restrict__ in, ChunkDesc d,
   br.in32 = reinterpret_cast<const uint32_t*>(in);
   // the window reads up to 128 bits (4 words) ahead of the decode position
   const uint64_t trunc_words = (d.in_end * 8 + 31) / 32 + 5;
-  br.limit_words = trunc_words;
-  if (d.abort_bit != kNoStop && d.abort_bit / 32 + 5 < trunc_words) br.limit_words = d.abort_bit / 32 + 5;
+  // the reader may run up to the abort bit (moved on by every extension)
+  auto set_limit = [&]() {
+    br.limit_words = (d.abort_bit != kNoStop && d.abort_bit / 32 + 5 < trunc_words)
+                         ? d.abort_bit / 32 + 5
+                         : trunc_words;
+  };
+  set_limit();
   br.load_windows((d.start_bit >> 5) & ~31ull, lane);
   br.seek(d.start_bit, lane);
   br.refill(lane);
@@ -814,6 +819,7 @@ __device__ int32_t decode_chunk(const uint8_t* __restrict__ in, ChunkDesc d,
       if (bitpos < nx_lo) {
         d.stop_lo = nx_lo;
         if (d.abort_bit != kNoStop) d.abort_bit = d.stop_lo + slack;
+        set_limit();
       } else {
         // a sync start is taken over only mid-block, at its exact symbol
         // start (huff_block_parallel); a block boundary at or past it
@@ -828,6 +834,7 @@ __device__ int32_t decode_chunk(const uint8_t* __restrict__ in, ChunkDesc d,
         }
         d.next = nx.next;
         extends++;
+        set_limit();
         if (bitpos >= d.stop_lo) continue;
       }
     }
