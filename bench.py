@@ -303,6 +303,145 @@ def bench_batch(args, rank: int, world: int, local: int):
         print(json.dumps(line), flush=True)
 
 
+def run_trace(srv, comps, sizes, crcs, arrivals, free, verify_every: int = 8):
+    """Replay arrivals (t, pool index) against a Server; returns per-request
+    (total_ms, queue_ms), wall seconds from the first arrival to the last
+    completion, and whether the sampled outputs matched."""
+    import threading
+    import zlib
+    import gzippy_b200 as G
+    lock = threading.Lock()        # free: pool index -> spare output buffers
+    tickets = [None] * len(arrivals)
+    t0 = time.perf_counter()
+
+    def submitter():
+        for k, (t, i) in enumerate(arrivals):
+            d = t0 + t - time.perf_counter()
+            if d > 0:
+                time.sleep(d)
+            with lock:
+                lst = free.setdefault(i, [])
+                out = lst.pop() if lst else np.empty(int(sizes[i]) + 64, np.uint8)
+            tickets[k] = (srv.submit(comps[i], out=out), i, out)
+
+    th = threading.Thread(target=submitter)
+    th.start()
+    lat, ok, n_checked = [], True, 0
+    for k in range(len(arrivals)):
+        while tickets[k] is None:
+            time.sleep(0.0005)
+        tk, i, out = tickets[k]
+        rc, data, tm = srv.poll(tk, -1, copy=False)
+        if rc != G.OK or len(data) != int(sizes[i]):
+            ok = False
+        elif k % verify_every == 0:
+            n_checked += 1
+            ok &= zlib.crc32(data) == crcs[i]
+        lat.append((tm.total_ms, tm.queue_ms))
+        with lock:
+            free.setdefault(i, []).append(out)
+    th.join()
+    wall = time.perf_counter() - t0
+    return lat, wall, ok, n_checked
+
+
+def bench_serving(args, rank: int, world: int, local: int):
+    """Serving: Poisson arrivals of mixed-size requests against the
+    continuous-batching Server, and the plain path (one request per call, in
+    arrival order) on the same trace."""
+    from gzippy_b200 import workloads as W
+    import gzippy_b200 as G
+    import torch
+    torch.cuda.set_device(local)
+    comps, sizes, crcs, specs = W.serving_pool(n=args.pool)
+    mean_req = float(np.mean(sizes))
+    cfg_base = {"workload": "serving", "pool_requests": len(comps), "seed": 1238,
+                "host_buffers": "page-locked inputs and outputs >= 1 MiB",
+                "sizes": "4-256 KiB log-uniform (p=0.8) or 8-512 MiB log-uniform",
+                "budget_bytes": 120 << 30, "lanes": args.lanes,
+                "parallelism": f"replicas x{world}"}
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        from concurrent.futures import ThreadPoolExecutor
+        from oracle import pyoracle as O
+        t0 = time.perf_counter()
+        with ThreadPoolExecutor(cpus()) as ex:
+            outs = list(ex.map(lambda c: O.decompress(c, cap=int(c[-4:].view("<u4")[0]) + 4096)[1].size, comps))
+        dt = time.perf_counter() - t0
+        v = sum(outs) / dt / 1e9
+        print(json.dumps({"metric": METRIC, "value": round(v, 4), "unit": "GB/s", "n_gpus": world,
+                          "steps": 1, "warmup": 0, "ms_per_step": round(dt * 1e3, 1),
+                          "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                          "dtype": "u8", "data": "synthetic", "config": cfg_base, "impl": "reference",
+                          "cpu_baseline": {"value": round(v, 4), "unit": "GB/s", "cores": cpus(),
+                                           "kind": "port", "sample": "the request pool once, one "
+                                           "request per task, oracle serial decoder"},
+                          "e2e": {"value": round(v, 4), "unit": "GB/s", "h2d_bytes_per_step": 0,
+                                  "d2h_bytes_per_step": 0}}), flush=True)
+        return
+    # host buffers page-locked, as a server's caller keeps them (the large
+    # ones then move by DMA without staging); small outputs stay pageable
+    comps = [torch.from_numpy(c).pin_memory().numpy() for c in comps]
+
+    def out_buf(i):
+        n = int(sizes[i]) + 64
+        return torch.empty(n, dtype=torch.uint8).pin_memory().numpy() if n >= (1 << 20) \
+            else np.empty(n, np.uint8)
+
+    free = {i: [out_buf(i), out_buf(i)] for i in range(len(comps))}
+
+    # capacity: the whole pool submitted at once to a server, after a warm-up pass
+    srv = G.Server(device=local, lanes=args.lanes)
+    for rep in range(2):
+        t0 = time.perf_counter()
+        tks = [srv.submit(c, out=free[i][0]) for i, c in enumerate(comps)]
+        for tk in tks:
+            srv.result(tk, copy=False)
+        cap_gbs = sum(sizes) / (time.perf_counter() - t0) / 1e9
+    srv.close()
+    rate = args.rate or 0.6 * cap_gbs * 1e9 / mean_req
+    arrivals = W.poisson_arrivals(1238, rate, args.duration, len(comps))
+    offered = sum(sizes[i] for _, i in arrivals)
+    res = {}
+    for mode in ("served", "plain"):
+        if mode == "served":
+            srv = G.Server(device=local, lanes=args.lanes)
+        else:
+            srv = G.Server(device=local, lanes=1, max_batch_requests=1)
+        # warm the lanes' buffers with one pass over the pool
+        for tk in [srv.submit(c, out=free[i][0]) for i, c in enumerate(comps)]:
+            srv.result(tk, copy=False)
+        with ClockSampler(local) as clk:
+            lat, wall, ok, n_checked = run_trace(srv, comps, sizes, crcs, arrivals, free)
+        st = srv.stats()
+        srv.close()
+        tot = np.array([x[0] for x in lat])
+        qw = np.array([x[1] for x in lat])
+        res[mode] = {"value": round(offered / wall / 1e9, 4), "unit": "GB/s",
+                     "p50_ms": round(float(np.percentile(tot, 50)), 3),
+                     "p99_ms": round(float(np.percentile(tot, 99)), 3),
+                     "p50_queue_ms": round(float(np.percentile(qw, 50)), 3),
+                     "p99_queue_ms": round(float(np.percentile(qw, 99)), 3),
+                     "requests": len(lat), "batches": int(st.batches), "byte_exact_sample": ok,
+                     "checked": n_checked, "wall_s": round(wall, 2), "clocks": clk.summary()}
+    line = {"metric": METRIC, "value": res["served"]["value"], "unit": "GB/s", "n_gpus": world,
+            "steps": 1, "warmup": 1, "ms_per_step": round(res["served"]["wall_s"] * 1e3, 1),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+            "data": "synthetic (seeded generator + zlib levels 1/6/9)",
+            "config": dict(cfg_base, rate_hz=round(rate, 2), duration_s=args.duration,
+                           batched_capacity_gbs=round(cap_gbs, 3),
+                           mean_request_bytes=int(mean_req), offered_bytes=int(offered)),
+            "p50_ms": res["served"]["p50_ms"], "p99_ms": res["served"]["p99_ms"],
+            "served": res["served"], "plain": res["plain"],
+            "e2e": {"value": res["served"]["value"], "unit": "GB/s",
+                    "h2d_bytes_per_step": int(sum(len(comps[i]) for _, i in arrivals)),
+                    "d2h_bytes_per_step": int(offered)},
+            "clocks": res["served"]["clocks"]}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 class ClockSampler:
     """nvidia-smi clocks / throttle reasons sampled every 200 ms."""
 
@@ -404,6 +543,10 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--rate", type=float, default=0.0, help="serving: arrivals/s (0 = 60%% of capacity)")
+    ap.add_argument("--duration", type=float, default=60.0, help="serving: seconds of arrivals")
+    ap.add_argument("--pool", type=int, default=64, help="serving: distinct requests")
+    ap.add_argument("--lanes", type=int, default=3, help="serving: concurrent batches")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -414,6 +557,8 @@ def main():
         args.warmup = 3
     if args.workload == "stream_batch":
         return bench_batch(args, rank, world, local)
+    if args.workload == "serving":
+        return bench_serving(args, rank, world, local)
 
     config = {"workload": args.workload, "streams": 1, "level": 6, "seed": 1235,
               "plain_bytes": None, "comp_bytes": None,

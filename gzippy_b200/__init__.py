@@ -29,11 +29,13 @@ import numpy as np
 from . import build as _build
 
 __all__ = ["GzippyError", "decompress", "decompress_with_threads", "decompress_to_writer",
-           "decompress_to_writer_with_threads", "decompress_batch", "Context", "Stats", "lib"]
+           "decompress_to_writer_with_threads", "decompress_batch", "Context", "Server", "Stats",
+           "lib"]
 
 OK, NOT_GZIP, BAD_HEADER, BAD_DEFLATE, CRC_MISMATCH, SIZE_MISMATCH, OUT_TOO_SMALL = range(7)
 DEVICE_ERROR, TIMEOUT, TRUNCATED, INVALID_ARGUMENT = 7, 8, 9, 12
 NOALLOC_TOO_LARGE = 14
+OVER_BUDGET, PENDING = 15, 16
 NOALLOC_MAX_OUT = 4 << 20
 
 
@@ -75,6 +77,26 @@ class Stats(ctypes.Structure):
         return {n: getattr(self, n) for n, _ in self._fields_}
 
 
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int), ("lanes", ctypes.c_int), ("autotune", ctypes.c_int),
+                ("pad", ctypes.c_int), ("budget_bytes", ctypes.c_size_t),
+                ("max_batch_bytes", ctypes.c_size_t), ("max_batch_requests", ctypes.c_size_t),
+                ("large_bytes", ctypes.c_size_t)]
+
+
+class RequestTimes(ctypes.Structure):
+    _fields_ = [("queue_ms", ctypes.c_double), ("total_ms", ctypes.c_double)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint64) for n in
+                ("submitted", "completed", "batches", "in_flight", "queued", "budget_used",
+                 "in_bytes", "out_bytes")]
+
+    def as_dict(self) -> dict:
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
 WRITE_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t)
 
 _lock = threading.Lock()
@@ -101,6 +123,13 @@ def lib():
             L.gzgpu_decompress_to_writer.argtypes = [vp, vp, sz, WRITE_FN, vp,
                                                      ctypes.POINTER(ctypes.c_uint64)]
             u64p = ctypes.POINTER(ctypes.c_uint64)
+            L.gzgpu_server_create.argtypes = [ctypes.POINTER(vp), ctypes.POINTER(ServerConfig)]
+            L.gzgpu_server_destroy.argtypes = [vp]
+            L.gzgpu_server_destroy.restype = None
+            L.gzgpu_submit.argtypes = [vp, vp, sz, vp, sz, u64p]
+            L.gzgpu_poll.argtypes = [vp, ctypes.c_uint64, ctypes.c_int, ctypes.POINTER(sz),
+                                     ctypes.POINTER(RequestTimes)]
+            L.gzgpu_server_get_stats.argtypes = [vp, ctypes.POINTER(ServerStats)]
             L.gzgpu_decompress_batch_device.argtypes = [vp, vp, u64p, u64p, sz, vp, sz, u64p, u64p,
                                                         ctypes.POINTER(ctypes.c_int)]
             L.gzgpu_decompress_batch.argtypes = [vp, ctypes.POINTER(Span), sz, ctypes.POINTER(Out),
@@ -383,6 +412,81 @@ def decompress_device_noalloc(d_in: int, in_len: int, d_out: int, out_cap: int,
             raise GzippyError("Decompression", f"output needs {n.value} bytes", rc)
         _raise(rc)
     return n.value
+
+
+class Server:
+    """Continuous-batching decompression service (gzgpu_server_*, no reference
+    counterpart).  submit() queues a gzip buffer and returns a ticket;
+    result() / poll() give its bytes.  Requests run in lanes (contexts with
+    their own CUDA streams) that overlap on the GPU, admitted against a
+    device-memory budget; small requests share batches."""
+
+    def __init__(self, device: int = 0, lanes: int = 3, budget_bytes: int = 0,
+                 max_batch_bytes: int = 0, max_batch_requests: int = 0, large_bytes: int = 0,
+                 autotune: bool = False):
+        self._lib = lib()
+        cfg = ServerConfig(device, lanes, int(autotune), 0, budget_bytes, max_batch_bytes,
+                           max_batch_requests, large_bytes)
+        h = ctypes.c_void_p()
+        rc = self._lib.gzgpu_server_create(ctypes.byref(h), ctypes.byref(cfg))
+        if rc != OK:
+            _raise(rc)
+        self._h = h
+        self._keep = {}  # ticket -> (input, output) arrays held until done
+
+    def close(self):
+        if self._h:
+            self._lib.gzgpu_server_destroy(self._h)
+            self._h = None
+            self._keep.clear()
+
+    def __del__(self):  # pragma: no cover
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit(self, data, out_cap: int | None = None, out: np.ndarray | None = None) -> int:
+        a = _as_u8(data)
+        if out is None:
+            if out_cap is None:
+                isize = int(a[-4:].view("<u4")[0]) if a.size >= 4 else 0
+                out_cap = max(isize, a.size * 4, 1 << 12)
+            out = np.empty(out_cap, np.uint8)
+        t = ctypes.c_uint64(0)
+        rc = self._lib.gzgpu_submit(self._h, a.ctypes.data, a.size, out.ctypes.data, out.size,
+                                    ctypes.byref(t))
+        if rc != OK:
+            _raise(rc)
+        self._keep[t.value] = (a, out)
+        return t.value
+
+    def poll(self, ticket: int, wait_ms: int = -1, copy: bool = True):
+        """(status, data or None, RequestTimes); status PENDING while running.
+        A finished ticket is released.  data is bytes, or with copy=False a
+        numpy view of the output buffer (no copy)."""
+        n = ctypes.c_size_t(0)
+        tm = RequestTimes()
+        rc = self._lib.gzgpu_poll(self._h, ticket, wait_ms, ctypes.byref(n), ctypes.byref(tm))
+        if rc == PENDING:
+            return rc, None, tm
+        _, out = self._keep.pop(ticket, (None, None))
+        if rc in (OK, NOT_GZIP):
+            if out is None:
+                return rc, (b"" if copy else np.empty(0, np.uint8)), tm
+            return rc, (out[:n.value].tobytes() if copy else out[:n.value]), tm
+        return rc, None, tm
+
+    def result(self, ticket: int, copy: bool = True):
+        rc, data, _ = self.poll(ticket, -1, copy)
+        if rc not in (OK, NOT_GZIP):
+            _raise(rc)
+        return data
+
+    def stats(self) -> ServerStats:
+        s = ServerStats()
+        self._lib.gzgpu_server_get_stats(self._h, ctypes.byref(s))
+        return s
 
 
 def decompress_batch(datas) -> list:

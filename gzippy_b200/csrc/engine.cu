@@ -21,6 +21,7 @@
 #include <map>
 #include <mutex>
 #include <new>
+#include <thread>
 #include <vector>
 
 #include "../../include/gzgpu.h"
@@ -34,21 +35,25 @@ using namespace gzgpu;
 
 namespace {
 
+// Device buffer that grows in stream order on its context's stream
+// (cudaMallocAsync / cudaFreeAsync): growing one context's buffers does not
+// synchronize the device, so contexts on other threads keep running.
 struct DevBuf {
   void* p = nullptr;
   size_t cap = 0;
+  cudaStream_t st = nullptr;
   cudaError_t ensure(size_t n) {
     if (n <= cap) return cudaSuccess;
-    if (p) cudaFree(p);
+    if (p) cudaFreeAsync(p, st);
     p = nullptr;
     cap = 0;
     size_t want = n + n / 4 + 4096;
-    cudaError_t e = cudaMalloc(&p, want);
+    cudaError_t e = cudaMallocAsync(&p, want, st);
     if (e == cudaSuccess) cap = want;
     return e;
   }
   void release() {
-    if (p) cudaFree(p);
+    if (p) cudaFreeAsync(p, st);
     p = nullptr;
     cap = 0;
   }
@@ -145,7 +150,9 @@ const char* kErrStr[] = {"ok",
                          "chunk not decoded",
                          "invalid argument",
                          "speculative chunk overshot its stop",
-                         "output exceeds the 4 MiB limit of the no-allocation entry point"};
+                         "output exceeds the 4 MiB limit of the no-allocation entry point",
+                         "request exceeds the server's device-memory budget",
+                         "request still pending"};
 
 }  // namespace
 
@@ -167,6 +174,11 @@ struct gzgpu_ctx {
   DevBuf pages, owner, seq, placed, placed_of, list, segs, cblocks, bcrcs, mblk, mtrail, mlen,
       mcrc, mstatus;
   HostPinned h_stage;
+  std::vector<DevBuf*> all_bufs() {
+    return {&in,     &out,   &s_off,   &s_len,  &info,   &units,   &cands,  &counters, &descs,
+            &results, &spec, &work,    &pages,  &owner,  &seq,     &placed, &placed_of, &list,
+            &segs,   &cblocks, &bcrcs, &mblk,   &mtrail, &mlen,    &mcrc,   &mstatus};
+  }
   const uint8_t* cur_in = nullptr;  // input buffer of the running job
   uint8_t* user_out = nullptr;       // caller device output (device-resident API)
   size_t user_cap = 0;
@@ -749,6 +761,7 @@ int gzgpu_ctx::run(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R) 
       // grow device arrays, preserving contents
       size_t ncap = (hd.size() + nr) * 2;
       DevBuf nd, nrr;
+      nd.st = nrr.st = st;
       if ((rc = check(nd.ensure(sizeof(ChunkDesc) * ncap))) ||
           (rc = check(nrr.ensure(sizeof(ChunkResult) * ncap))))
         return rc;
@@ -999,6 +1012,15 @@ int gzgpu_create(gzgpu_ctx** out, const gzgpu_config* cfg) {
     return GZGPU_DEVICE_ERROR;
   }
   for (auto& e : c->ev) cudaEventCreate(&e);
+  for (DevBuf* b : c->all_bufs()) b->st = c->st;
+  {
+    // keep memory freed by buffer growth in the device's pool for reuse
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, c->dev) == cudaSuccess) {
+      uint64_t keep = ~0ull;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+  }
   c->setup_decode_grid();
   *out = c;
   return GZGPU_OK;
@@ -1008,12 +1030,8 @@ void gzgpu_destroy(gzgpu_ctx* c) {
   if (!c) return;
   cudaSetDevice(c->dev);
   cudaStreamSynchronize(c->st);
-  DevBuf* bufs[] = {&c->in,     &c->out,   &c->s_off,   &c->s_len,  &c->info,   &c->units,
-                    &c->cands,  &c->counters, &c->descs, &c->results, &c->spec, &c->work,
-                    &c->pages,  &c->owner, &c->seq,     &c->placed, &c->placed_of, &c->list,
-                    &c->segs,   &c->cblocks, &c->bcrcs, &c->mblk,   &c->mtrail, &c->mlen,
-                    &c->mcrc,   &c->mstatus};
-  for (DevBuf* b : bufs) b->release();
+  for (DevBuf* b : c->all_bufs()) b->release();
+  cudaStreamSynchronize(c->st);
   c->h_stage.release();
   for (auto& e : c->ev) cudaEventDestroy(e);
   cudaStreamDestroy(c->st);
@@ -1190,6 +1208,60 @@ int gzgpu_decompress_batch_device(gzgpu_ctx* c, const void* d_in, const uint64_t
   return all;
 }
 
+namespace {
+
+// Host copies of the batch path: a stream of at least kDirectBytes in
+// page-locked memory moves by DMA straight from / to the caller's buffer;
+// the others go through the context's pinned staging buffer, copied by up
+// to kCopyThreads host threads.
+constexpr size_t kDirectBytes = 1u << 20;
+constexpr int kCopyThreads = 8;
+
+bool host_pinned(const void* p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();  // pageable memory of an old driver reports an error: clear it
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+
+struct CopyJob {
+  void* dst;
+  const void* src;
+  size_t len;
+};
+
+void parallel_copy(const std::vector<CopyJob>& jobs) {
+  size_t total = 0;
+  for (const CopyJob& j : jobs) total += j.len;
+  int nt = (int)std::min<size_t>(kCopyThreads, total / (8u << 20) + 1);
+  nt = std::max(1, std::min(nt, (int)std::thread::hardware_concurrency()));
+  if (nt <= 1) {
+    for (const CopyJob& j : jobs) memcpy(j.dst, j.src, j.len);
+    return;
+  }
+  // split the byte range evenly; a job may be cut between threads
+  const size_t per = (total + nt - 1) / nt;
+  std::vector<std::thread> th;
+  for (int t = 0; t < nt; t++) {
+    th.emplace_back([&, t] {
+      const size_t b0 = t * per, b1 = std::min(total, b0 + per);
+      size_t at = 0;
+      for (const CopyJob& j : jobs) {
+        const size_t j0 = at, j1 = at + j.len;
+        at = j1;
+        if (j1 <= b0 || j0 >= b1) continue;
+        const size_t s0 = std::max(j0, b0) - j0, s1 = std::min(j1, b1) - j0;
+        memcpy((uint8_t*)j.dst + s0, (const uint8_t*)j.src + s0, s1 - s0);
+      }
+    });
+  }
+  for (std::thread& x : th) x.join();
+}
+
+}  // namespace
+
 int gzgpu_decompress_batch(gzgpu_ctx* c, const gzgpu_span* ins, size_t n, gzgpu_out* outs,
                            int* statuses) {
   if (!c || (n && (!ins || !outs || !statuses))) return GZGPU_INVALID_ARGUMENT;
@@ -1200,38 +1272,66 @@ int gzgpu_decompress_batch(gzgpu_ctx* c, const gzgpu_span* ins, size_t n, gzgpu_
   for (size_t i = 0; i < n; i++) total += (ins[i].len + 15) & ~15ull;
   int rc;
   if ((rc = c->check(c->in.ensure(total + kInputPad)))) return rc;
-  // pack the streams (16-byte aligned) through the pinned bounce buffer
-  if (!c->h_stage.ensure(total ? total : 1)) return GZGPU_DEVICE_ERROR;
-  uint8_t* hb = reinterpret_cast<uint8_t*>(c->h_stage.p);
+  // pack the streams (16-byte aligned): staged ones into the pinned buffer
   std::vector<StreamSpec> S(n);
-  uint64_t at = 0;
+  std::vector<char> direct(n, 0);
+  std::vector<CopyJob> jobs;
+  uint64_t at = 0, staged = 0;
   for (size_t i = 0; i < n; i++) {
-    if (ins[i].len) memcpy(hb + at, ins[i].data, ins[i].len);
     S[i] = StreamSpec{at, ins[i].len};
+    direct[i] = ins[i].len >= kDirectBytes && host_pinned(ins[i].data);
+    if (!direct[i]) staged += ins[i].len;
     at += (ins[i].len + 15) & ~15ull;
   }
+  // runs of consecutive staged streams: each is laid out in the staging
+  // buffer as on the device and uploaded by one copy
+  struct Run {
+    size_t i, j;
+    uint64_t stage_off;
+  };
+  std::vector<Run> runs;
+  uint64_t stage_total = 0;
+  for (size_t i = 0; i < n;) {
+    if (direct[i]) {
+      i++;
+      continue;
+    }
+    size_t j = i;
+    while (j < n && !direct[j]) j++;
+    runs.push_back(Run{i, j, stage_total});
+    stage_total += S[j - 1].off + S[j - 1].len - S[i].off;
+    i = j;
+  }
+  if (!c->h_stage.ensure(stage_total ? stage_total : 1)) return GZGPU_DEVICE_ERROR;
+  uint8_t* hb = reinterpret_cast<uint8_t*>(c->h_stage.p);
+  for (const Run& r : runs)
+    for (size_t k = r.i; k < r.j; k++)
+      if (ins[k].len)
+        jobs.push_back(CopyJob{hb + r.stage_off + (S[k].off - S[r.i].off), ins[k].data, ins[k].len});
+  parallel_copy(jobs);
   cudaEventRecord(c->ev[0], c->st);
-  if (at && (rc = c->check(cudaMemcpyAsync(c->in.p, hb, at, cudaMemcpyHostToDevice, c->st))))
-    return rc;
-  cudaMemsetAsync(c->in.as<uint8_t>() + at, 0, kInputPad, c->st);
-  c->cur_in = c->in.as<uint8_t>();
+  uint8_t* din = c->in.as<uint8_t>();
+  for (size_t i = 0; i < n; i++)
+    if (direct[i])
+      cudaMemcpyAsync(din + S[i].off, ins[i].data, ins[i].len, cudaMemcpyHostToDevice, c->st);
+  for (const Run& r : runs) {
+    const uint64_t r0 = S[r.i].off, r1 = S[r.j - 1].off + S[r.j - 1].len;
+    if (r1 > r0 && (rc = c->check(cudaMemcpyAsync(din + r0, hb + r.stage_off, r1 - r0,
+                                                  cudaMemcpyHostToDevice, c->st))))
+      return rc;
+  }
+  cudaMemsetAsync(din + at, 0, kInputPad, c->st);
+  c->cur_in = din;
   c->user_out = nullptr;
   std::vector<StreamOut> R;
   rc = c->job(S, R);
   if (rc != kOk) return rc;
   finish_stats(c);
   int all = GZGPU_OK;
-  uint64_t out_total = 0;
-  for (size_t i = 0; i < n; i++) out_total += R[i].out_len;
-  if (!c->h_stage.ensure(out_total ? out_total : 1)) return GZGPU_DEVICE_ERROR;
-  hb = reinterpret_cast<uint8_t*>(c->h_stage.p);
   cudaEvent_t t0 = c->ev[8], t1 = c->ev[9];
   cudaEventRecord(t0, c->st);
-  if (out_total && (rc = c->check(cudaMemcpyAsync(hb, c->cur_out, out_total, cudaMemcpyDeviceToHost,
-                                                  c->st))))
-    return rc;
-  cudaEventRecord(t1, c->st);
-  if ((rc = c->check(cudaStreamSynchronize(c->st)))) return rc;
+  jobs.clear();
+  std::vector<char> deliver(n, 0);
   for (size_t i = 0; i < n; i++) {
     statuses[i] = R[i].status;
     outs[i].len = R[i].status == kOk ? R[i].out_len : 0;
@@ -1239,10 +1339,46 @@ int gzgpu_decompress_batch(gzgpu_ctx* c, const gzgpu_span* ins, size_t n, gzgpu_
       statuses[i] = GZGPU_OUT_TOO_SMALL;
       outs[i].len = R[i].out_len;
     } else if (R[i].status == kOk && R[i].out_len) {
-      memcpy(outs[i].data, hb + R[i].out_off, R[i].out_len);
+      deliver[i] = 1;
     }
     if (statuses[i] != GZGPU_OK && statuses[i] != GZGPU_NOT_GZIP && all == GZGPU_OK) all = statuses[i];
   }
+  // outputs: large ones into page-locked caller memory by DMA; the rest in
+  // runs contiguous on the device, one download each into the staging buffer
+  std::vector<char> odirect(n, 0);
+  runs.clear();
+  stage_total = 0;
+  for (size_t i = 0; i < n; i++)
+    odirect[i] = deliver[i] && R[i].out_len >= kDirectBytes && host_pinned(outs[i].data);
+  for (size_t i = 0; i < n;) {
+    if (!deliver[i] || odirect[i]) {
+      i++;
+      continue;
+    }
+    size_t j = i + 1;
+    while (j < n && deliver[j] && !odirect[j] && R[j].out_off == R[j - 1].out_off + R[j - 1].out_len)
+      j++;
+    runs.push_back(Run{i, j, stage_total});
+    stage_total += R[j - 1].out_off + R[j - 1].out_len - R[i].out_off;
+    i = j;
+  }
+  if (!c->h_stage.ensure(stage_total ? stage_total : 1)) return GZGPU_DEVICE_ERROR;
+  hb = reinterpret_cast<uint8_t*>(c->h_stage.p);
+  for (size_t i = 0; i < n; i++)
+    if (odirect[i])
+      cudaMemcpyAsync(outs[i].data, c->cur_out + R[i].out_off, R[i].out_len, cudaMemcpyDeviceToHost,
+                      c->st);
+  for (const Run& r : runs) {
+    const uint64_t r0 = R[r.i].out_off, r1 = R[r.j - 1].out_off + R[r.j - 1].out_len;
+    if ((rc = c->check(cudaMemcpyAsync(hb + r.stage_off, c->cur_out + r0, r1 - r0,
+                                       cudaMemcpyDeviceToHost, c->st))))
+      return rc;
+    for (size_t k = r.i; k < r.j; k++)
+      jobs.push_back(CopyJob{outs[k].data, hb + r.stage_off + (R[k].out_off - r0), R[k].out_len});
+  }
+  cudaEventRecord(t1, c->st);
+  if ((rc = c->check(cudaStreamSynchronize(c->st)))) return rc;
+  parallel_copy(jobs);
   float t = 0;
   cudaEventElapsedTime(&t, t0, t1);
   c->stats.ms_d2h = t;

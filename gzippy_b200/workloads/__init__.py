@@ -201,3 +201,41 @@ def serving_requests(seed: int = 1238, rate_hz: float = 20.0, duration_s: float 
         size = int(np.exp(rng.uniform(np.log(lo), np.log(hi))))
         out.append((t, size, int(rng.integers(0, 4)), int(rng.choice([1, 6, 9]))))
     return out
+
+
+def serving_pool(seed: int = 1238, n: int = 64, small=(4 << 10, 256 << 10),
+                 large=(8 << 20, 512 << 20), p_small=0.8, threads: int | None = None):
+    """n distinct serving requests: uncompressed size log-uniform in `small`
+    with probability p_small, else log-uniform in `large`; content type
+    uniform over the four kinds, level uniform in {1, 6, 9}.  Returns
+    (compressed arrays, plain sizes, plain CRC32s, specs)."""
+    import zlib
+    rng = np.random.default_rng(seed)
+    specs = []
+    for i in range(n):
+        lo, hi = small if rng.random() < p_small else large
+        size = int(np.exp(rng.uniform(np.log(lo), np.log(hi))))
+        specs.append((size, int(rng.integers(0, 4)), int(rng.choice([1, 6, 9]))))
+    comps, crcs = [None] * n, [0] * n
+
+    def one(i):
+        size, ctype, level = specs[i]
+        p = content(ctype, seed * 7907 + i, size)
+        comps[i] = gzip_member(p, level)
+        crcs[i] = zlib.crc32(p)
+
+    with ThreadPoolExecutor(threads or _cpus()) as ex:
+        list(ex.map(one, range(n)))
+    return comps, [s[0] for s in specs], crcs, specs
+
+
+def poisson_arrivals(seed: int, rate_hz: float, duration_s: float, n_pool: int):
+    """Arrival times of a Poisson process over duration_s, each with a pool index."""
+    rng = np.random.default_rng(seed)
+    t, out = 0.0, []
+    while True:
+        t += rng.exponential(1.0 / rate_hz)
+        if t >= duration_s:
+            return out
+        out.append((t, int(rng.integers(0, n_pool))))
+

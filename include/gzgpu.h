@@ -41,6 +41,8 @@ extern "C" {
 #define GZGPU_TRUNCATED 9
 #define GZGPU_INVALID_ARGUMENT 12
 #define GZGPU_NOALLOC_TOO_LARGE 14 /* output beyond GZGPU_NOALLOC_MAX_OUT */
+#define GZGPU_OVER_BUDGET 15 /* request larger than the server's device-memory budget */
+#define GZGPU_PENDING 16     /* gzgpu_poll: the request has not finished */
 
 /* readable bytes the device-resident entry point needs after the input */
 #define GZGPU_INPUT_PAD 1024
@@ -158,6 +160,52 @@ int gzgpu_decompress_batch_device(gzgpu_ctx *ctx, const void *d_in, const uint64
 #define GZGPU_NOALLOC_MAX_OUT (4u << 20)
 int gzgpu_decompress_device_noalloc(const void *d_in, size_t in_len, void *d_out, size_t out_cap,
                                     size_t *out_len, void *cuda_stream);
+
+/* Serving (no reference counterpart): a continuous-batching service over
+ * host buffers.  Requests are submitted from any thread and decoded by
+ * `lanes` worker threads, each with its own context (CUDA stream and device
+ * buffers kept between batches), so batches overlap on the GPU.  A request
+ * is admitted when its charge (compressed size + 3 x out_cap + 1 MiB: output
+ * and decoder pages) fits the device-memory budget next to the requests in
+ * flight; the queue is FIFO.  A request of at least large_bytes compressed
+ * runs alone; smaller ones are merged, up to max_batch_bytes of input, into
+ * one batch (one gzgpu_decompress_batch job).  Inputs and outputs are the
+ * caller's and must stay valid until the request has been polled done. */
+typedef struct gzgpu_server gzgpu_server;
+
+typedef struct {
+  int device;
+  int lanes;                 /* concurrent batches; 0 = 3 */
+  int autotune;              /* the lanes' contexts use the autotuner */
+  int pad;
+  size_t budget_bytes;       /* device-memory budget of admitted requests; 0 = 120 GB */
+  size_t max_batch_bytes;    /* compressed bytes merged into one batch; 0 = 256 MiB */
+  size_t max_batch_requests; /* requests merged into one batch; 0 = 4096 */
+  size_t large_bytes;        /* compressed size from which a request runs alone; 0 = 32 MiB */
+} gzgpu_server_config;
+
+typedef struct {
+  double queue_ms;  /* submit -> admitted to a lane */
+  double total_ms;  /* submit -> decoded (host output written) */
+} gzgpu_request_times;
+
+typedef struct {
+  uint64_t submitted, completed, batches, in_flight, queued, budget_used, in_bytes, out_bytes;
+} gzgpu_server_stats;
+
+int gzgpu_server_create(gzgpu_server **out, const gzgpu_server_config *cfg);
+/* Waits for running batches; requests still queued are dropped. */
+void gzgpu_server_destroy(gzgpu_server *srv);
+/* Queue one gzip buffer; *ticket identifies it.  GZGPU_OVER_BUDGET when its
+ * charge alone exceeds the budget. */
+int gzgpu_submit(gzgpu_server *srv, const uint8_t *in, size_t in_len, uint8_t *out,
+                 size_t out_cap, uint64_t *ticket);
+/* GZGPU_PENDING while the request runs (wait_ms: 0 = return at once, < 0 =
+ * wait until done, > 0 = wait at most that long); then its status (as
+ * gzgpu_decompress), *out_len and its times, and the ticket is released. */
+int gzgpu_poll(gzgpu_server *srv, uint64_t ticket, int wait_ms, size_t *out_len,
+               gzgpu_request_times *times);
+int gzgpu_server_get_stats(gzgpu_server *srv, gzgpu_server_stats *out);
 
 /* Diagnostics (no reference counterpart; used by the parity tests).
  *
