@@ -136,7 +136,8 @@ def lib():
                                                  ctypes.POINTER(ctypes.c_int)]
             L.gzgpu_get_stats.argtypes = [vp, ctypes.POINTER(Stats)]
             L.gzgpu_debug_find.argtypes = [vp, vp, sz, vp, vp, sz, vp, vp, vp]
-            L.gzgpu_debug_decode.argtypes = [vp, vp, sz, vp, vp, vp, sz, vp, sz, vp]
+            L.gzgpu_debug_decode.argtypes = [vp, vp, sz, vp, vp, vp, sz, vp, sz, vp, vp]
+            L.gzgpu_debug_dyn_sync.argtypes = [vp, vp, sz, vp, vp, vp, sz, vp, vp]
             L.gzgpu_debug_last_chunks.argtypes = [vp, vp, vp, sz, ctypes.POINTER(sz)]
             L.gzgpu_decompress_device_noalloc.argtypes = [vp, sz, vp, sz, ctypes.POINTER(sz), vp]
             _lib = L
@@ -298,7 +299,23 @@ class Context:
         return [None if not va[i] else ((int(lo[i]), int(hi[i])) if va[i] == 1 else ("sync", int(lo[i])))
                 for i in range(n)]
 
-    def debug_decode(self, data, chunks, cap_per):
+    def debug_dyn_sync(self, data, items):
+        """Dynamic sync-start search on [(table_bit, from_bit, to_bit)] -> bit or None each."""
+        a = _as_u8(data)
+        n = len(items)
+        tb = np.array([x[0] for x in items], np.uint64)
+        fr = np.array([x[1] for x in items], np.uint64)
+        to = np.array([x[2] for x in items], np.uint64)
+        out = np.zeros(n, np.uint64)
+        va = np.zeros(n, np.int32)
+        rc = self._lib.gzgpu_debug_dyn_sync(self._h, a.ctypes.data, a.size, tb.ctypes.data,
+                                            fr.ctypes.data, to.ctypes.data, n, out.ctypes.data,
+                                            va.ctypes.data)
+        if rc != OK:
+            _raise(rc)
+        return [int(out[i]) if va[i] else None for i in range(n)]
+
+    def debug_decode(self, data, chunks, cap_per, tables=None):
         """Inflate kernel on explicit chunks [(start_bit, stop_bit, flags)], flags bit 0 =
         member start, bit 1 = sync start.  Returns (results n x 7 uint64: end_bit,
         out_len, marker_end, n_blocks, status, final_block, sync_end; entries n x
@@ -310,22 +327,23 @@ class Context:
         mf = np.array([int(c[2]) for c in chunks], np.int32)
         ent = np.zeros((n, cap_per), np.uint16)
         res = np.zeros((n, 7), np.uint64)
+        tb = np.array(tables if tables is not None else [0] * n, np.uint64)
         rc = self._lib.gzgpu_debug_decode(self._h, a.ctypes.data, a.size, st.ctypes.data,
                                           sp.ctypes.data, mf.ctypes.data, n, ent.ctypes.data,
-                                          cap_per, res.ctypes.data)
+                                          cap_per, res.ctypes.data, tb.ctypes.data)
         if rc != OK:
             _raise(rc)
         return res, ent
 
     DESC_DTYPE = np.dtype([("start_bit", "<u8"), ("lo_bit", "<u8"), ("stop_lo", "<u8"),
                            ("guess_bit", "<u8"), ("limit_bit", "<u8"), ("in_end", "<u8"),
-                           ("abort_bit", "<u8"), ("flags", "<u4"), ("stream", "<u4"),
-                           ("next", "<u4"), ("pad", "<u4")])
+                           ("abort_bit", "<u8"), ("table_bit", "<u8"), ("flags", "<u4"),
+                           ("stream", "<u4"), ("next", "<u4"), ("est_ratio", "<f4")])
     RESULT_DTYPE = np.dtype([("end_bit", "<u8"), ("out_len", "<u8"), ("marker_end", "<u8"),
                              ("last_page", "<u4"), ("prev_page", "<u4"), ("n_pages", "<u4"),
                              ("n_blocks", "<u4"), ("status", "<i4"), ("final_block", "<i4"),
                              ("t_start", "<u8"), ("t_end", "<u8"), ("gen", "<u4"),
-                             ("sync_end", "<u4")])
+                             ("sync_end", "<u4"), ("end_hdr_bit", "<u8")])
 
     def last_chunks(self):
         """(descs, results) structured arrays of the last job's chunk table."""

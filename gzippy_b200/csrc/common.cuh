@@ -44,8 +44,10 @@ enum : uint32_t {
   kChunkMemberFirst = 1u,  // starts a member: zero window, never emits markers
   kChunkValid = 2u,        // has a start (member start or a finder candidate)
   kChunkConfirmed = 4u,    // starts at a boundary the chain walk confirmed (a repair)
-  kChunkSync = 8u,         // starts at a symbol boundary inside a non-final fixed-Huffman
-                           // block (a sync start), not at a block header
+  kChunkSync = 8u,         // a sync start: a symbol boundary inside a Huffman block, not
+                           // a block header (table_bit: that block's header; 0 = a
+                           // non-final fixed-Huffman block)
+  kChunkPiece = 16u,       // a piece of a partition cut by its output estimate
 };
 
 // Sync starts in fixed-Huffman data: positions are walked from kSyncOffsets
@@ -53,6 +55,8 @@ enum : uint32_t {
 // from + kSyncOffsets + kSyncSpan.
 constexpr uint32_t kSyncOffsets = 64;
 constexpr uint64_t kSyncSpan = 8192;
+constexpr uint64_t kSyncSpanDyn = 16384;  // walk length inside a dynamic block
+constexpr uint64_t kSyncMinSlack = 1ull << 16;  // least run past its stop of a sync start
 constexpr uint64_t kSyncFail = ~0ull;
 
 struct ChunkDesc {
@@ -63,10 +67,11 @@ struct ChunkDesc {
   uint64_t limit_bit;  // end of the finder's search range
   uint64_t in_end;     // byte end of this chunk's stream in the input buffer
   uint64_t abort_bit;  // a speculative chunk gives up past this bit (kNoStop = never)
+  uint64_t table_bit;  // sync start: header bit of its block (0 = fixed code, or none)
   uint32_t flags;
   uint32_t stream;     // stream id
   uint32_t next;       // index of the next valid chunk of the stream (kNoChunk = none)
-  uint32_t pad;
+  float est_ratio;     // finder's estimate of output bytes per input byte (0 = none)
 };
 constexpr uint32_t kNoChunk = 0xFFFFFFFFu;
 // phantom successors a speculative chunk decodes through; a chunk whose start
@@ -86,6 +91,7 @@ struct ChunkResult {
   uint64_t t_start, t_end;  // %globaltimer (ns) when the warp took / finished the chunk
   uint32_t gen;             // decode attempt that produced this result (page tag)
   uint32_t sync_end;        // 1: stopped at its successor's sync start (mid-block)
+  uint64_t end_hdr_bit;     // sync_end: header bit of the block it stopped in (0 = fixed)
 };
 
 // a page's seq word: attempt (gen) in the top 8 bits, page index below

@@ -254,6 +254,8 @@ struct gzgpu_ctx {
 
 // shortest partition of a high-ratio member (8 KiB of compressed input)
 constexpr uint64_t kMinPartitionBits = 8ull << 13;
+// shortest piece of a partition cut by the output estimate (4 KiB of input)
+constexpr uint64_t kMinPieceBits = 4ull << 13;
 
 static uint64_t pick_chunk_bytes(uint64_t in_len) {
   // about two chunks per decoding warp on large inputs; smaller chunks for
@@ -488,8 +490,7 @@ int gzgpu_ctx::run(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R) 
     }
     c1[s] = (uint32_t)hd.size();
   }
-  const uint32_t n_grid = (uint32_t)hd.size();
-  stats.n_chunks = n_grid;
+  uint32_t n_grid = (uint32_t)hd.size();
   size_t desc_cap = n_grid + 4096;
   if ((rc = check(descs.ensure(sizeof(ChunkDesc) * desc_cap))) ||
       (rc = check(results.ensure(sizeof(ChunkResult) * desc_cap))) ||
@@ -504,11 +505,95 @@ int gzgpu_ctx::run(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R) 
   if ((rc = check(launch_finder(cur_in, descs.as<ChunkDesc>(), spec.as<uint32_t>(),
                                 (uint32_t)hspec.size(), st))))
     return rc;
+  stats.kernel_launches += 2;
+  // ---- 3a. cut high-ratio partitions finer ---------------------------------
+  // A chunk's decode time follows its output; the finder estimated each
+  // dynamic start's output per input byte from its code lengths.  Partitions
+  // expected to produce more than twice 2 x chunk_bytes are cut into pieces
+  // of about that output, which get their own finder pass.
+  if (!hspec.empty()) {
+    if ((rc = check(cudaMemcpyAsync(hd.data(), descs.p, sizeof(ChunkDesc) * n_grid,
+                                    cudaMemcpyDeviceToHost, st))) ||
+        (rc = check(cudaStreamSynchronize(st))))
+      return rc;
+    const double target = 2.0 * (double)cb;
+    std::vector<ChunkDesc> hd2;
+    std::vector<uint32_t> newpos(n_grid + 1), hspec2;
+    hd2.reserve(n_grid + n_grid / 4);
+    for (uint32_t i = 0; i < n_grid; i++) {
+      newpos[i] = (uint32_t)hd2.size();
+      hd2.push_back(hd[i]);
+      const ChunkDesc& p = hd[i];
+      if (!(p.flags & kChunkValid) || (p.flags & (kChunkMemberFirst | kChunkSync)) ||
+          !(p.est_ratio > 0.f) || p.limit_bit <= p.start_bit)
+        continue;
+      // the first block may not represent the partition (a content change
+      // inside it): the next partition's first block shows its far end
+      float ratio = p.est_ratio;
+      if (i + 1 < n_grid && hd[i + 1].stream == p.stream && (hd[i + 1].flags & kChunkValid) &&
+          !(hd[i + 1].flags & kChunkMemberFirst))
+        ratio = std::max(ratio, hd[i + 1].est_ratio);
+      const uint64_t span = p.limit_bit - p.start_bit;
+      const double est = (double)ratio * (double)span / 8.0;
+      if (est <= 2.0 * target) continue;
+      const uint64_t k = std::min<uint64_t>(8, (uint64_t)(est / target + 0.999));
+      const uint64_t piece = std::max<uint64_t>((span / k) & ~63ull, kMinPieceBits);
+      for (uint64_t g = p.start_bit + piece; g + kMinPieceBits <= p.limit_bit; g += piece) {
+        ChunkDesc x{};
+        x.start_bit = x.lo_bit = x.guess_bit = g;
+        x.limit_bit = std::min(g + piece, p.limit_bit);
+        if (p.limit_bit - x.limit_bit < kMinPieceBits) x.limit_bit = p.limit_bit;
+        x.stop_lo = kNoStop;
+        x.in_end = p.in_end;
+        x.stream = p.stream;
+        x.flags = kChunkPiece;
+        hspec2.push_back((uint32_t)hd2.size());
+        hd2.push_back(x);
+        if (x.limit_bit == p.limit_bit) break;
+      }
+    }
+    newpos[n_grid] = (uint32_t)hd2.size();
+    if (!hspec2.empty()) {
+      for (uint32_t s = 0; s < ns; s++) {
+        c0[s] = newpos[c0[s]];
+        c1[s] = newpos[c1[s]];
+        for (uint32_t& m : mc0[s]) m = newpos[m];
+      }
+      hd.swap(hd2);
+      n_grid = (uint32_t)hd.size();
+      desc_cap = n_grid + 4096;
+      if ((rc = check(descs.ensure(sizeof(ChunkDesc) * desc_cap))) ||
+          (rc = check(results.ensure(sizeof(ChunkResult) * desc_cap))) ||
+          (rc = check(spec.ensure(4 * (hspec2.size() + 1)))) ||
+          (rc = check(work.ensure(4 * desc_cap))))
+        return rc;
+      cudaMemcpyAsync(descs.p, hd.data(), sizeof(ChunkDesc) * n_grid, cudaMemcpyHostToDevice, st);
+      cudaMemcpyAsync(spec.p, hspec2.data(), 4 * hspec2.size(), cudaMemcpyHostToDevice, st);
+      if ((rc = check(launch_finder(cur_in, descs.as<ChunkDesc>(), spec.as<uint32_t>(),
+                                    (uint32_t)hspec2.size(), st))))
+        return rc;
+      stats.kernel_launches += 2;
+    }
+    // sync starts inside dynamic blocks for every partition still empty
+    std::vector<uint32_t> hsync;
+    hsync.reserve(n_grid);
+    for (uint32_t i = 0; i < n_grid; i++)
+      if (!(hd[i].flags & kChunkMemberFirst)) hsync.push_back(i);
+    if (!hsync.empty()) {
+      if ((rc = check(spec.ensure(4 * (hsync.size() + 1))))) return rc;
+      cudaMemcpyAsync(spec.p, hsync.data(), 4 * hsync.size(), cudaMemcpyHostToDevice, st);
+      if ((rc = check(launch_dyn_sync(cur_in, descs.as<ChunkDesc>(), spec.as<uint32_t>(),
+                                      (uint32_t)hsync.size(), st))))
+        return rc;
+      stats.kernel_launches += 1;
+    }
+  }
+  stats.n_chunks = n_grid;
   if ((rc = check(launch_link(descs.as<ChunkDesc>(), n_grid, work.as<uint32_t>(),
                               counters.as<uint32_t>() + 1, std::max<uint64_t>(cbits, 1ull << 21),
                               st))))
     return rc;
-  stats.kernel_launches += 2;
+  stats.kernel_launches += 1;
   cudaEventRecord(ev[4], st);
   // ---- 4. decode ----------------------------------------------------------
   uint64_t pages_needed = (est_out + n_grid * (uint64_t)kPageEntries) / kPageEntries + 64;
@@ -582,7 +667,8 @@ int gzgpu_ctx::run(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R) 
   // a repair starts at a confirmed boundary and stops at the start of grid
   // chunk `next` (kNoChunk: none); like a member-first chunk it decodes on
   // through any phantom successors it finds there
-  auto new_chunk = [&](Walker& w, uint64_t start, uint64_t stop, uint32_t flags, uint32_t next) {
+  auto new_chunk = [&](Walker& w, uint64_t start, uint64_t stop, uint32_t flags, uint32_t next,
+                       uint64_t table_bit = 0) {
     ChunkDesc d{};
     d.start_bit = d.lo_bit = d.guess_bit = d.limit_bit = start;
     if (flags & kChunkMemberFirst) d.limit_bit = S[w.stream].off + w.mpos;
@@ -592,6 +678,7 @@ int gzgpu_ctx::run(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R) 
     d.flags = flags | kChunkValid | kChunkConfirmed;
     d.stream = w.stream;
     d.next = next;
+    d.table_bit = table_bit;
     uint32_t id = (uint32_t)(hd.size() + repairs.size());
     repairs.push_back(d);
     repair_owner.push_back(w.stream);
@@ -724,7 +811,7 @@ int gzgpu_ctx::run(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R) 
         // optimistic: the repair ends at the next candidate's start
         Walker::Checkpoint cp{w.order.size(), w.members.size(), j, w.member,
                               w.member_order_begin, w.mpos};
-        new_chunk(w, e, stop, r.sync_end ? kChunkSync : 0u, j);
+        new_chunk(w, e, stop, r.sync_end ? kChunkSync : 0u, j, r.sync_end ? r.end_hdr_bit : 0);
         uint32_t rid = (uint32_t)w.pending;
         w.pending = -1;
         w.assumed.push_back(Walker::Assumption{rid, hd[j].lo_bit, hd[j].start_bit, is_sync(j), cp});
@@ -733,7 +820,8 @@ int gzgpu_ctx::run(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R) 
         w.j = j + 1;
         continue;
       }
-      new_chunk(w, e, stop, r.sync_end ? kChunkSync : 0u, j < w.c1 ? j : kNoChunk);
+      new_chunk(w, e, stop, r.sync_end ? kChunkSync : 0u, j < w.c1 ? j : kNoChunk,
+                r.sync_end ? r.end_hdr_bit : 0);
       break;
     }
   };
@@ -1427,9 +1515,58 @@ int gzgpu_debug_find(gzgpu_ctx* c, const uint8_t* in, size_t in_len, const uint6
   return GZGPU_OK;
 }
 
+int gzgpu_debug_dyn_sync(gzgpu_ctx* c, const uint8_t* in, size_t in_len, const uint64_t* table_bit,
+                         const uint64_t* from, const uint64_t* to, size_t n, uint64_t* out,
+                         int* valid) {
+  if (!c || (!in && in_len) || (n && (!table_bit || !from || !to || !out || !valid)))
+    return GZGPU_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> g(c->mu);
+  cudaSetDevice(c->dev);
+  int rc;
+  if ((rc = c->check(c->in.ensure(in_len + kInputPad))) ||
+      (rc = c->check(c->descs.ensure(sizeof(ChunkDesc) * (2 * n + 1)))) ||
+      (rc = c->check(c->spec.ensure(4 * (n + 1)))))
+    return rc;
+  cudaMemcpyAsync(c->in.p, in, in_len, cudaMemcpyHostToDevice, c->st);
+  cudaMemsetAsync(c->in.as<uint8_t>() + in_len, 0, kInputPad, c->st);
+  // each range is a piece after a parent whose start is the block's header
+  std::vector<ChunkDesc> d(2 * n);
+  std::vector<uint32_t> pieces(n);
+  for (size_t i = 0; i < n; i++) {
+    ChunkDesc& p = d[2 * i];
+    p = ChunkDesc{};
+    p.start_bit = p.lo_bit = p.guess_bit = table_bit[i];
+    p.limit_bit = from[i];
+    p.in_end = in_len;
+    p.flags = kChunkValid;
+    ChunkDesc& q = d[2 * i + 1];
+    q = ChunkDesc{};
+    q.start_bit = q.lo_bit = q.guess_bit = from[i];
+    q.limit_bit = to[i];
+    q.in_end = in_len;
+    q.flags = kChunkPiece;
+    pieces[i] = (uint32_t)(2 * i + 1);
+  }
+  if (n) {
+    cudaMemcpyAsync(c->descs.p, d.data(), sizeof(ChunkDesc) * 2 * n, cudaMemcpyHostToDevice, c->st);
+    cudaMemcpyAsync(c->spec.p, pieces.data(), 4 * n, cudaMemcpyHostToDevice, c->st);
+    if ((rc = c->check(launch_dyn_sync(c->in.as<uint8_t>(), c->descs.as<ChunkDesc>(),
+                                       c->spec.as<uint32_t>(), (uint32_t)n, c->st))))
+      return rc;
+    cudaMemcpyAsync(d.data(), c->descs.p, sizeof(ChunkDesc) * 2 * n, cudaMemcpyDeviceToHost, c->st);
+  }
+  if ((rc = c->check(cudaStreamSynchronize(c->st)))) return rc;
+  for (size_t i = 0; i < n; i++) {
+    const ChunkDesc& q = d[2 * i + 1];
+    valid[i] = (q.flags & kChunkValid) ? 1 : 0;
+    out[i] = valid[i] ? q.start_bit : 0;
+  }
+  return GZGPU_OK;
+}
+
 int gzgpu_debug_decode(gzgpu_ctx* c, const uint8_t* in, size_t in_len, const uint64_t* start,
                        const uint64_t* stop, const int* flags, size_t n, uint16_t* entries,
-                       size_t cap_per, uint64_t* res) {
+                       size_t cap_per, uint64_t* res, const uint64_t* table_bit) {
   if (!c || (!in && in_len) || (n && (!start || !stop || !flags || !res)))
     return GZGPU_INVALID_ARGUMENT;
   std::lock_guard<std::mutex> g(c->mu);
@@ -1457,6 +1594,7 @@ int gzgpu_debug_decode(gzgpu_ctx* c, const uint8_t* in, size_t in_len, const uin
     d[i].in_end = in_len;
     d[i].flags = kChunkValid | ((flags[i] & 1) ? kChunkMemberFirst : 0u) |
                  ((flags[i] & 2) ? kChunkSync : 0u);
+    d[i].table_bit = table_bit ? table_bit[i] : 0;
     wl[i] = (uint32_t)i;
   }
   // a chunk followed by a sync start may stop at it mid-block

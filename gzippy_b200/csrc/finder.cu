@@ -62,6 +62,9 @@ __global__ void __launch_bounds__(32 * kFinderWarps)
       d.lo_bit = hit_lo[bwarp];
       d.start_bit = hit_hi[bwarp];
       d.flags |= kChunkValid;
+      // BTYPE at the start: 2 = dynamic (estimate from its code lengths), 0 = stored
+      const uint32_t bt = (uint32_t)(peek_bits(in, nbytes, d.start_bit, 3) >> 1);
+      d.est_ratio = bt == 2 ? dyn_header_ratio(in, nbytes, d.start_bit) : 1.f;
     } else {
       d.flags &= ~kChunkValid;
     }
@@ -142,7 +145,14 @@ __global__ void link_kernel(ChunkDesc* descs, uint32_t n, uint32_t* work, uint32
   }
   d.stop_lo = stop;
   d.next = next;
-  d.abort_bit = (stop != kNoStop && !(d.flags & kChunkMemberFirst)) ? stop + slack : kNoStop;
+  // A sync start whose table or alignment is wrong decodes garbage that a
+  // complete code never rejects: it may run at most its own length (at least
+  // kSyncMinSlack) past its stop.  A real one stops at its successor, or goes
+  // by phantom successors mid-block to the one after (inflate.cu).
+  uint64_t s = slack;
+  if ((d.flags & kChunkSync) && stop != kNoStop && stop > d.start_bit)
+    s = min(slack, max(stop - d.start_bit, (uint64_t)kSyncMinSlack));
+  d.abort_bit = (stop != kNoStop && !(d.flags & kChunkMemberFirst)) ? stop + s : kNoStop;
   work[atomicAdd(n_work, 1u)] = i;
 }
 

@@ -351,4 +351,101 @@ static __device__ uint64_t fixed_walk(const uint32_t* sw, uint64_t wbase, uint64
 // words a sync search from `from` stages: [from >> 5, (target + 96) >> 5] + 1
 constexpr uint32_t kSyncWords = (uint32_t)((kSyncOffsets + kSyncSpan + 96 + 64) / 32) + 2;
 
+// ---------------------------------------------------------------------------
+// Expected output bytes per compressed byte of the dynamic block whose header
+// starts at `bit` (a candidate the finder accepted), from its code lengths
+// alone: a code of length L stands for a symbol of probability 2^-L.
+// Literals give one byte, a length symbol its mean length; a symbol costs its
+// code, its extra bits and, for a length, the mean distance code and extra
+// bits.  Used to cut high-ratio partitions finer (no reference counterpart).
+// ---------------------------------------------------------------------------
+static __constant__ uint16_t f_len_base[29] = {3,  4,  5,  6,  7,  8,  9,  10, 11,  13,
+                                               15, 17, 19, 23, 27, 31, 35, 43, 51,  59,
+                                               67, 83, 99, 115, 131, 163, 195, 227, 258};
+
+static __device__ __noinline__ float dyn_header_ratio(const uint8_t* in, uint64_t nbytes,
+                                                      uint64_t bit) {
+  const uint32_t h = (uint32_t)peek_bits(in, nbytes, bit, 17);
+  const int hl = 257 + ((h >> 3) & 31), hd = 1 + ((h >> 8) & 31), pc = ((h >> 13) & 15) + 4;
+  const uint64_t pbits = peek_bits(in, nbytes, bit + 17, 3 * pc);
+  uint8_t cl[19];
+  for (int i = 0; i < 19; i++) cl[i] = 0;
+  for (int i = 0; i < pc; i++) cl[f_cl_order[i]] = (uint8_t)((pbits >> (3 * i)) & 7);
+  uint16_t cnt[8], first[8], offs[8];
+  uint8_t sorted[19];
+  for (int L = 0; L < 8; L++) cnt[L] = 0;
+  for (int s = 0; s < 19; s++) cnt[cl[s]]++;
+  cnt[0] = 0;
+  {
+    uint32_t code = 0, off = 0;
+    for (int L = 1; L < 8; L++) {
+      if (L > 1) code = (code + cnt[L - 1]) << 1;
+      first[L] = (uint16_t)code;
+      offs[L] = (uint16_t)off;
+      off += cnt[L];
+    }
+    uint16_t nx[8];
+    for (int L = 0; L < 8; L++) nx[L] = offs[L];
+    for (int s = 0; s < 19; s++)
+      if (cl[s]) sorted[nx[cl[s]]++] = (uint8_t)s;
+  }
+  float out = 0.f, bits = 0.f, len_p = 0.f, dist_bits = 0.f, dist_p = 0.f;
+  uint64_t pos = bit + 17 + 3 * pc;
+  const int total = hl + hd;
+  uint32_t prev = 0;
+  for (int i = 0; i < total;) {
+    const uint32_t rev = __brev((uint32_t)peek_bits(in, nbytes, pos, 14)) >> 25;
+    int sym = -1;
+    for (int L = 1; L < 8; L++) {
+      const uint32_t idx = (rev >> (7 - L)) - first[L];
+      if (idx < cnt[L]) {
+        sym = sorted[offs[L] + idx];
+        pos += L;
+        break;
+      }
+    }
+    if (sym < 0) return 0.f;
+    uint32_t v = (uint32_t)sym;
+    int rep = 1;
+    if (sym == 16) {
+      v = prev;
+      rep = 3 + (int)peek_bits(in, nbytes, pos, 2);
+      pos += 2;
+    } else if (sym == 17) {
+      v = 0;
+      rep = 3 + (int)peek_bits(in, nbytes, pos, 3);
+      pos += 3;
+    } else if (sym == 18) {
+      v = 0;
+      rep = 11 + (int)peek_bits(in, nbytes, pos, 7);
+      pos += 7;
+    }
+    if (v) {
+      const float p = __int_as_float((127 - (int)v) << 23);  // 2^-v
+      for (int k = i; k < i + rep && k < total; k++) {
+        if (k < 256) {
+          out += p;
+          bits += p * (float)v;
+        } else if (k >= 257 && k < hl && k < 286) {
+          const int li = k - 257;
+          len_p += p;
+          out += p * ((float)f_len_base[li] + 0.5f * (float)((1u << f_len_extra[li]) - 1));
+          bits += p * (float)(v + f_len_extra[li]);
+        } else if (k >= hl) {
+          const int di = k - hl;
+          if (di < 30) {
+            dist_p += p;
+            dist_bits += p * (float)(v + f_dist_extra[di]);
+          }
+        }
+      }
+    }
+    prev = v;
+    i += rep;
+  }
+  if (dist_p > 0.f) bits += len_p * dist_bits / dist_p;
+  return bits > 0.f ? 8.f * out / bits : 0.f;
+}
+
 }  // namespace gzgpu
+

@@ -536,7 +536,8 @@ __device__ int32_t huff_block_parallel(BitReader& br, const Tables<LB>* T, PageH
                                        const PagePool& pool, uint32_t cid, uint32_t gen,
                                        uint64_t& o, uint64_t& guard, uint64_t& marker_end,
                                        bool zero_window, uint64_t trunc_words,
-                                       uint64_t sync_target, bool& synced, int lane) {
+                                       uint64_t sync_target, uint64_t passed_bit, bool& synced,
+                                       bool& passed, int lane) {
   constexpr uint32_t LMASK = (1u << LB) - 1, DMASK = (1u << kDistBits) - 1;
   uint64_t pos = br.pos();
   int32_t status = kOk;
@@ -732,6 +733,11 @@ __device__ int32_t huff_block_parallel(BitReader& br, const Tables<LB>* T, PageH
       break;
     }
     if (eob) break;
+    // the successor's start went by mid-block: it can never be handed over
+    if (passed_bit < pos) {
+      passed = true;
+      break;
+    }
   }
   br.seek(pos, lane);
   br.refill(lane);
@@ -797,12 +803,32 @@ __device__ int32_t decode_chunk(const uint8_t* __restrict__ in, ChunkDesc d,
 
   int extends = 0;
   const uint64_t slack = d.abort_bit != kNoStop ? d.abort_bit - d.stop_lo : 0;
-  // a sync start begins inside a non-final fixed-Huffman block (no header)
-  bool in_fixed_block = (d.flags & kChunkSync) != 0;
+  // a sync start begins inside a block: the Huffman block whose header is at
+  // d.table_bit, or (table_bit 0) a non-final fixed-Huffman block
+  bool in_sync_block = (d.flags & kChunkSync) != 0;
   bool synced = false;
+  uint64_t blk_hdr = 0;  // header bit of the block being decoded (0 = unknown)
+  uint32_t bfinal = 0, btype = 0;
+  bool resume = false;  // continue the current block after going by a successor
+  const bool confirmed = (d.flags & (kChunkMemberFirst | kChunkConfirmed)) != 0;
+  // move on past successor d.next (a phantom)
+  auto extend = [&](const ChunkDesc& nx) {
+    if (nx.next == kNoChunk) {
+      d.stop_lo = kNoStop;
+      d.abort_bit = kNoStop;
+    } else {
+      d.stop_lo = handover_bit(descs[nx.next]);
+      if (d.abort_bit != kNoStop) d.abort_bit = d.stop_lo + slack;
+    }
+    d.next = nx.next;
+    extends++;
+    set_limit();
+  };
   for (;;) {
     uint64_t bitpos = br.pos();
-    if (bitpos >= d.stop_lo) {
+    const bool resume_now = resume;
+    resume = false;
+    if (!resume_now && bitpos >= d.stop_lo) {
       // A block boundary past the successor's start range means that start
       // was a phantom: decode on to the start after it (the consumer's
       // re-decode from the confirmed boundary, chunk_fetcher.rs:855).
@@ -838,6 +864,16 @@ __device__ int32_t decode_chunk(const uint8_t* __restrict__ in, ChunkDesc d,
         if (bitpos >= d.stop_lo) continue;
       }
     }
+    if (resume_now) {
+      // successors whose start this chunk is already past, mid-block
+      while (d.next != kNoChunk && (confirmed || extends < kMaxExtends)) {
+        const ChunkDesc nx = descs[d.next];
+        if ((nx.flags & kChunkMemberFirst) ||
+            ((const volatile ChunkDesc*)(descs + d.next))->start_bit >= bitpos)
+          break;
+        extend(nx);
+      }
+    }
     if (bitpos > d.abort_bit) {
       status = kOvershoot;
       break;
@@ -846,12 +882,37 @@ __device__ int32_t decode_chunk(const uint8_t* __restrict__ in, ChunkDesc d,
       status = kTruncated;
       break;
     }
-    uint32_t bfinal, btype;
-    if (in_fixed_block) {
-      in_fixed_block = false;
-      bfinal = 0;
-      btype = 1;
+    bool tables_ready = resume_now;
+    if (resume_now) {
+      // same block, tables in place
+    } else if (in_sync_block) {
+      in_sync_block = false;
+      if (d.table_bit) {
+        // the block's own header: type, BFINAL and code tables; then back
+        // to the sync start
+        br.seek(d.table_bit, lane);
+        br.refill(lane);
+        const uint32_t hdr = (uint32_t)br.bb & 7;
+        br.consume(3);
+        bfinal = hdr & 1;
+        btype = hdr >> 1;
+        if (btype != 1 && btype != 2) {
+          status = kBadDeflate;
+          break;
+        }
+        status = read_tables<LB>(br, btype, T, trunc_words, lane);
+        if (status != kOk) break;
+        tables_ready = true;
+        blk_hdr = d.table_bit;
+        br.seek(d.start_bit, lane);
+        br.refill(lane);
+      } else {
+        bfinal = 0;
+        btype = 1;
+        blk_hdr = 0;
+      }
     } else {
+      blk_hdr = bitpos;
       br.refill(lane);
       const uint32_t hdr = (uint32_t)br.bb & 7;
       br.consume(3);
@@ -901,19 +962,35 @@ __device__ int32_t decode_chunk(const uint8_t* __restrict__ in, ChunkDesc d,
       guard = 0;
       br.seek((byte + ln) * 8, lane);
     } else if (btype == 1 || btype == 2) {
-      status = read_tables<LB>(br, btype, T, trunc_words, lane);
+      if (!tables_ready) status = read_tables<LB>(br, btype, T, trunc_words, lane);
       if (status != kOk) break;
       if (!kRing) {
-        // the successor's sync start can be taken over inside a non-final
-        // fixed block only (the state a sync start assumes)
-        uint64_t sync_target = kNoStop;
-        if (btype == 1 && !bfinal && d.next != kNoChunk) {
+        // the successor's sync start can be taken over only in the state
+        // it assumes: inside its block (same header), or inside a non-final
+        // fixed block for a fixed sync start.  Any successor whose start
+        // goes by mid-block is a phantom (real starts are block boundaries
+        // or sync starts reached exactly): the decode moves on past it.
+        uint64_t sync_target = kNoStop, passed_bit = kNoStop;
+        if (d.next != kNoChunk) {
           const ChunkDesc& nx = descs[d.next];
-          if (nx.flags & kChunkSync) sync_target = nx.start_bit;
+          if (nx.flags & kChunkSync) {
+            const bool same = nx.table_bit ? (blk_hdr == nx.table_bit)
+                                           : (btype == 1 && !bfinal);
+            if (same) sync_target = nx.start_bit;
+          }
+          if (!(nx.flags & kChunkMemberFirst) && (confirmed || extends < kMaxExtends))
+            passed_bit = ((const volatile ChunkDesc*)(descs + d.next))->start_bit;
         }
+        bool passed = false;
         status = huff_block_parallel<LB>(br, T, ph, pool, cid, gen, o, guard, marker_end,
-                                         zero_window, trunc_words, sync_target, synced, lane);
+                                         zero_window, trunc_words, sync_target, passed_bit, synced,
+                                         passed, lane);
         if (status != kOk || synced) break;
+        if (passed) {
+          extend(descs[d.next]);
+          resume = true;
+          continue;
+        }
         n_blocks++;
         if (bfinal) {
           final_block = 1;
@@ -1069,6 +1146,7 @@ __device__ int32_t decode_chunk(const uint8_t* __restrict__ in, ChunkDesc d,
     res->final_block = final_block;
     res->gen = gen;
     res->sync_end = synced ? 1u : 0u;
+    res->end_hdr_bit = synced ? blk_hdr : 0;
   }
   __syncwarp();
   return status;
@@ -1206,6 +1284,110 @@ int inflate_blocks_per_sm(bool ring, int ctas) {
 GZGPU_INST(10)
 GZGPU_INST(11)
 GZGPU_INST(12)
+
+// ---------------------------------------------------------------------------
+// Sync starts inside dynamic blocks (no counterpart in the reference).  A
+// partition (or piece) that the finder left without a start lies inside some
+// block; the nearest regular start before it in its stream names that
+// block's header (when a block start went unrecorded in between, the table is
+// wrong, the walks fail or agree on a false start, and no predecessor ever
+// hands over to it).  Warp 0 builds the block's code tables; each of
+// the kSyncOffsets threads walks the code's symbol positions from one start
+// bit to the first boundary at or past from + kSyncOffsets + kSyncSpanDyn
+// (an EOB or an invalid code fails the walk); the end most walks agree on (at
+// least two, ties to the lower bit) becomes the piece's start.  As with the
+// fixed-code sync starts, the predecessor decides: it hands over only on
+// reaching that bit as a symbol start inside the same block.
+// ---------------------------------------------------------------------------
+constexpr uint32_t kSyncScan = 256;  // chunks looked back for a block header
+
+__global__ void __launch_bounds__(kSyncOffsets)
+    dyn_sync_kernel(const uint8_t* __restrict__ in, ChunkDesc* descs,
+                    const uint32_t* __restrict__ pieces, uint32_t n) {
+  constexpr int LB = 10;
+  __shared__ Tables<LB> T;
+  __shared__ uint64_t ends[kSyncOffsets];
+  __shared__ uint64_t table;
+  __shared__ int ok;
+  if (blockIdx.x >= n) return;
+  const uint32_t j = pieces[blockIdx.x];
+  ChunkDesc& d = descs[j];
+  if (d.flags & kChunkValid) return;
+  const uint64_t from = d.guess_bit, to = d.limit_bit, nbytes = d.in_end;
+  const uint64_t target = from + kSyncOffsets + kSyncSpanDyn;
+  if (target + 64 > to || target + 128 > nbytes * 8) return;
+  if (threadIdx.x == 0) {
+    // nearest regular (non-sync) start before this range in its stream;
+    // chunks other CTAs turn into sync starts meanwhile are skipped like the
+    // invalid ones they were
+    uint64_t t = 0;
+    for (int64_t k = (int64_t)j - 1; k >= 0 && k + (int64_t)kSyncScan >= (int64_t)j; k--) {
+      const ChunkDesc& p = descs[k];
+      if (p.stream != d.stream) break;
+      const uint32_t f = p.flags;
+      if ((f & kChunkValid) && !(f & kChunkSync)) {
+        if (p.start_bit < from && (peek_bits(in, p.in_end, p.start_bit, 3) >> 1) == 2)
+          t = p.start_bit;
+        break;
+      }
+    }
+    table = t;
+    ok = 0;
+  }
+  __syncthreads();
+  if (!table) return;
+  const int lane = threadIdx.x & 31;
+  const uint64_t trunc_words = (nbytes * 8 + 31) / 32 + 5;
+  if (threadIdx.x < 32) {
+    BitReader br;
+    br.in32 = reinterpret_cast<const uint32_t*>(in);
+    br.limit_words = trunc_words;
+    br.load_windows(((table + 3) >> 5) & ~31ull, lane);
+    br.seek(table + 3, lane);
+    br.refill(lane);
+    const int32_t st = read_tables<LB>(br, 2, &T, trunc_words, lane);
+    if (lane == 0) ok = st == kOk;
+  }
+  __syncthreads();
+  if (!ok) return;
+  uint64_t p = from + threadIdx.x, e = kSyncFail;
+  while (p < target) {
+    uint32_t dist = 0;
+    const uint32_t info = decode_symbol_full<LB>(peek_bits(in, nbytes, p, 48), &T, &dist);
+    const uint32_t kind = (info >> 6) & 3;
+    if (kind == kKindBad || kind == kKindEob) break;
+    p += info & 63;
+    if (p >= target) e = p;
+  }
+  ends[threadIdx.x] = e;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint64_t best = kSyncFail;
+    uint32_t best_n = 1;
+    for (uint32_t i = 0; i < kSyncOffsets; i++) {
+      const uint64_t v = ends[i];
+      if (v == kSyncFail) continue;
+      uint32_t c = 0;
+      for (uint32_t k = 0; k < kSyncOffsets; k++) c += ends[k] == v;
+      if (c > best_n || (c == best_n && best != kSyncFail && v < best)) {
+        best = v;
+        best_n = c;
+      }
+    }
+    if (best != kSyncFail) {
+      d.lo_bit = d.start_bit = best;
+      d.table_bit = table;
+      d.flags |= kChunkValid | kChunkSync;
+    }
+  }
+}
+
+cudaError_t launch_dyn_sync(const uint8_t* in, ChunkDesc* descs, const uint32_t* pieces, uint32_t n,
+                            cudaStream_t stream) {
+  if (!n) return cudaSuccess;
+  dyn_sync_kernel<<<n, kSyncOffsets, 0, stream>>>(in, descs, pieces, n);
+  return cudaGetLastError();
+}
 
 // ===========================================================================
 // Decode without allocating: gzgpu_decompress_device_noalloc.

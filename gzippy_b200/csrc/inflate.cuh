@@ -21,5 +21,8 @@ cudaError_t launch_inflate(bool ring, int ctas, const uint8_t* in, ChunkDesc* de
                            ChunkResult* results, const uint32_t* work, const uint32_t* n_work,
                            uint32_t* work_counter, const PagePool& pool, int blocks,
                            cudaStream_t stream);
+// sync starts inside dynamic blocks for the listed pieces left without a start
+cudaError_t launch_dyn_sync(const uint8_t* in, ChunkDesc* descs, const uint32_t* pieces, uint32_t n,
+                            cudaStream_t stream);
 
 }  // namespace gzgpu

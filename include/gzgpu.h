@@ -218,23 +218,32 @@ int gzgpu_server_get_stats(gzgpu_server *srv, gzgpu_server_stats *out);
  *
  * gzgpu_debug_decode: run the inflate kernel on n explicit chunks (start
  * bit, stop bit, flags[i]: bit 0 = member start (zero window instead of
- * markers), bit 1 = sync start) and copy each chunk's u16 entries to
- * entries + i*cap_per.  A chunk followed by sync starts may stop at them
- * mid-block.  res[7*i..] = end_bit, out_len, marker_end, n_blocks, status,
+ * markers), bit 1 = sync start, inside the block whose header is at
+ * table_bit[i] (NULL or 0 = a fixed block)) and copy each chunk's u16
+ * entries to entries + i*cap_per.  A chunk followed by sync starts may stop
+ * at them mid-block.  res[7*i..] = end_bit, out_len, marker_end, n_blocks, status,
  * final_block, sync_end.  Mirrors decode_chunk
  * (src/decompress/parallel/chunk_decode.rs:225). */
 int gzgpu_debug_find(gzgpu_ctx *ctx, const uint8_t *in, size_t in_len, const uint64_t *from,
                      const uint64_t *to, size_t n, uint64_t *lo, uint64_t *hi, int *valid);
 int gzgpu_debug_decode(gzgpu_ctx *ctx, const uint8_t *in, size_t in_len, const uint64_t *start,
                        const uint64_t *stop, const int *flags, size_t n, uint16_t *entries,
-                       size_t cap_per, uint64_t *res);
+                       size_t cap_per, uint64_t *res, const uint64_t *table_bit);
+/* gzgpu_debug_dyn_sync: the dynamic sync-start search for n ranges
+ * [from[i], to[i]) inside the block whose header is at table_bit[i]; out[i]
+ * = the start found, valid[i] = 1 when one was found. */
+int gzgpu_debug_dyn_sync(gzgpu_ctx *ctx, const uint8_t *in, size_t in_len, const uint64_t *table_bit,
+                         const uint64_t *from, const uint64_t *to, size_t n, uint64_t *out,
+                         int *valid);
 
 /* gzgpu_debug_last_chunks: the chunk table of the last job.  descs holds
- * n records of 72 bytes (start_bit, lo_bit, stop_lo, guess_bit, limit_bit,
- * in_end, abort_bit as u64; flags, stream, next, pad as u32); results n records of 72
- * bytes (end_bit, out_len, marker_end as u64; last_page, prev_page, n_pages,
- * n_blocks as u32; status, final_block as i32; t_start, t_end as u64 device
- * nanoseconds; gen, sync_end as u32: 72 bytes).  *n = records available (copies min(cap, *n)). */
+ * n records of 80 bytes (start_bit, lo_bit, stop_lo, guess_bit, limit_bit,
+ * in_end, abort_bit, table_bit as u64; flags, stream, next as u32,
+ * est_ratio as f32); results n records of 80 bytes (end_bit, out_len,
+ * marker_end as u64; last_page, prev_page, n_pages, n_blocks as u32;
+ * status, final_block as i32; t_start, t_end as u64 device nanoseconds;
+ * gen, sync_end as u32; end_hdr_bit as u64).  *n = records available
+ * (copies min(cap, *n)). */
 int gzgpu_debug_last_chunks(gzgpu_ctx *ctx, void *descs, void *results, size_t cap, size_t *n);
 
 /* Statistics of the last call. */

@@ -361,24 +361,27 @@ int orc_dynamic_lengths(const uint8_t *data, size_t n, uint64_t bit, uint8_t *le
 /* ------------------------------------------------------------------------ */
 /* Core of orc_inflate_chunk, with the two modes of the device decoder's
  * sync starts (no counterpart in the reference):
- *   ORC_START_FIXED: start_bit is a symbol start inside a non-final
- *     fixed-Huffman block (no header is read for the first block);
+ *   ORC_START_SYNC: start_bit is a symbol start inside the Huffman block
+ *     whose header is at start_table (0: a non-final fixed-Huffman block);
  *   sync targets: the chunk's successors are sync starts t[0] < t[1] < ...;
- *     while decoding a non-final fixed block the chunk stops at the symbol
- *     start == t[k] of its current successor k (*sync_end = 1).  At a block
- *     boundary at or past t[k] it has gone by successor k and moves on to
- *     k + 1; past the last one it stops only at the final block.
+ *     inside successor k's block (or a non-final fixed block, for a fixed
+ *     sync start) the chunk stops at the symbol start == t[k]
+ *     (*sync_end = 1).  Once it is past t[k], mid-block or at a block
+ *     boundary, it has gone by successor k and moves on to k + 1; past the
+ *     last one it stops only at the final block.
  * Without targets the stop rule is the first block boundary >= stop_lo. */
 static int inflate_core(const uint8_t *data, size_t n, uint64_t start_bit, uint64_t stop_lo,
-                        int flags, const uint64_t *targets, size_t n_targets, int window_mode,
+                        int flags, uint64_t start_table, const uint64_t *targets,
+                        const uint64_t *target_tables, size_t n_targets, int window_mode,
                         const uint8_t *window, size_t wlen, uint16_t *out, size_t cap,
-                        orc_chunk_result *res, uint32_t *sync_end) {
+                        orc_chunk_result *res, uint32_t *sync_end, uint64_t *end_hdr) {
   pthread_once(&fixed_once, fixed_init);
   br_t b = {data, n, start_bit};
   uint64_t o = 0, marker_end = 0;
   uint32_t nblocks = 0, nbt[3] = {0, 0, 0};
   int final_block = 0, st = ORC_OK, synced = 0;
-  int in_fixed = (flags & ORC_START_FIXED) != 0;
+  int in_sync = (flags & ORC_START_SYNC) != 0, tables_ready = 0;
+  uint64_t blk_hdr = 0; /* header bit of the block being decoded (0 = unknown: a fixed sync start) */
   size_t cur = 0;
   htab_t *lit = NULL, *dist = NULL;
   htab_t *dyn = (htab_t *)malloc(2 * sizeof(htab_t));
@@ -394,16 +397,46 @@ static int inflate_core(const uint8_t *data, size_t n, uint64_t start_bit, uint6
     }
     if (b.pos >= stop_lo) break;
     int bfinal, btype;
-    if (in_fixed) {
-      in_fixed = 0;
-      bfinal = 0;
-      btype = 1;
+    tables_ready = 0;
+    if (in_sync) {
+      in_sync = 0;
+      if (start_table) {
+        /* the block's own header gives its type, BFINAL and code tables */
+        br_t hb = {data, n, start_table};
+        uint32_t hdr = (uint32_t)br_read(&hb, 3);
+        bfinal = hdr & 1;
+        btype = hdr >> 1;
+        if (btype == 1) {
+          lit = &fixed_lit;
+          dist = &fixed_dist;
+        } else if (btype == 2) {
+          lit = &dyn[0];
+          dist = &dyn[1];
+          int e = read_dynamic(&hb, lit, dist);
+          if (e) { st = e; break; }
+        } else {
+          st = ORC_BAD_DEFLATE;
+          break;
+        }
+        tables_ready = 1;
+        blk_hdr = start_table;
+      } else {
+        bfinal = 0;
+        btype = 1;
+        blk_hdr = 0;
+      }
     } else {
+      blk_hdr = b.pos;
       uint32_t hdr = (uint32_t)br_read(&b, 3);
       bfinal = hdr & 1;
       btype = hdr >> 1;
     }
-    const uint64_t watch = (btype == 1 && !bfinal && cur < n_targets) ? targets[cur] : (uint64_t)-1;
+    uint64_t watch = (uint64_t)-1;
+    if (cur < n_targets) {
+      const uint64_t tt = target_tables ? target_tables[cur] : 0;
+      const int same = tt ? (blk_hdr == tt) : (btype == 1 && !bfinal);
+      if (same) watch = targets[cur];
+    }
     if (br_over(&b)) { st = ORC_TRUNCATED; break; }
     if (btype == 0) {
       b.pos = (b.pos + 7) & ~7ull;
@@ -417,7 +450,9 @@ static int inflate_core(const uint8_t *data, size_t n, uint64_t start_bit, uint6
       for (uint32_t i = 0; i < len; i++) out[o++] = data[byte + 4 + i];
       b.pos += 8ull * (4 + len);
     } else if (btype == 1 || btype == 2) {
-      if (btype == 1) {
+      if (tables_ready) {
+        /* read from the block's header above */
+      } else if (btype == 1) {
         lit = &fixed_lit;
         dist = &fixed_dist;
       } else {
@@ -428,6 +463,15 @@ static int inflate_core(const uint8_t *data, size_t n, uint64_t start_bit, uint6
       }
       for (;;) {
         if (b.pos == watch) { synced = 1; break; }
+        if (cur < n_targets && b.pos > targets[cur]) {
+          /* went by a successor mid-block: a phantom; watch the next one */
+          while (cur < n_targets && b.pos > targets[cur]) cur++;
+          watch = (uint64_t)-1;
+          if (cur < n_targets) {
+            const uint64_t tt = target_tables ? target_tables[cur] : 0;
+            if (tt ? (blk_hdr == tt) : (btype == 1 && !bfinal)) watch = targets[cur];
+          }
+        }
         if (br_over(&b)) { st = ORC_TRUNCATED; break; }
         int sym = htab_decode(lit, &b);
         if (sym < 0) { st = ORC_BAD_DEFLATE; break; }
@@ -478,6 +522,7 @@ static int inflate_core(const uint8_t *data, size_t n, uint64_t start_bit, uint6
   }
   free(dyn);
   if (sync_end) *sync_end = (uint32_t)synced;
+  if (end_hdr) *end_hdr = synced ? blk_hdr : 0;
   res->end_bit = b.pos;
   res->out_len = o;
   res->marker_end = marker_end;
@@ -493,16 +538,18 @@ static int inflate_core(const uint8_t *data, size_t n, uint64_t start_bit, uint6
 int orc_inflate_chunk(const uint8_t *data, size_t n, uint64_t start_bit, uint64_t stop_lo,
                       int window_mode, const uint8_t *window, size_t wlen, uint16_t *out,
                       size_t cap, orc_chunk_result *res) {
-  return inflate_core(data, n, start_bit, stop_lo, 0, NULL, 0, window_mode, window, wlen, out,
-                      cap, res, NULL);
+  return inflate_core(data, n, start_bit, stop_lo, 0, 0, NULL, NULL, 0, window_mode, window, wlen,
+                      out, cap, res, NULL, NULL);
 }
 
 int orc_inflate_chunk_ex(const uint8_t *data, size_t n, uint64_t start_bit, uint64_t stop_lo,
-                         int flags, const uint64_t *sync_targets, size_t n_targets,
-                         uint16_t *out, size_t cap, orc_chunk_result *res, uint32_t *sync_end) {
-  return inflate_core(data, n, start_bit, stop_lo, flags, sync_targets, n_targets,
-                      (flags & ORC_ZERO_WINDOW) ? ORC_WIN_BYTES : ORC_WIN_MARKERS, NULL, 0, out,
-                      cap, res, sync_end);
+                         int flags, uint64_t start_table, const uint64_t *sync_targets,
+                         const uint64_t *target_tables, size_t n_targets, uint16_t *out,
+                         size_t cap, orc_chunk_result *res, uint32_t *sync_end,
+                         uint64_t *end_hdr) {
+  return inflate_core(data, n, start_bit, stop_lo, flags, start_table, sync_targets, target_tables,
+                      n_targets, (flags & ORC_ZERO_WINDOW) ? ORC_WIN_BYTES : ORC_WIN_MARKERS,
+                      NULL, 0, out, cap, res, sync_end, end_hdr);
 }
 
 /* ------------------------------------------------------------------------ */
@@ -552,6 +599,54 @@ int orc_fixed_sync_find(const uint8_t *data, size_t n, uint64_t from, uint64_t t
   if (target + 64 > to || target + 128 > (uint64_t)n * 8) return 0;
   uint64_t e[ORC_SYNC_OFFSETS];
   for (int i = 0; i < ORC_SYNC_OFFSETS; i++) e[i] = fixed_walk(data, n, from + i, target);
+  uint64_t best = SYNC_FAIL;
+  int best_n = 1;
+  for (int i = 0; i < ORC_SYNC_OFFSETS; i++) {
+    if (e[i] == SYNC_FAIL) continue;
+    int c = 0;
+    for (int j = 0; j < ORC_SYNC_OFFSETS; j++) c += e[j] == e[i];
+    if (c > best_n || (c == best_n && best != SYNC_FAIL && e[i] < best)) {
+      best = e[i];
+      best_n = c;
+    }
+  }
+  if (best == SYNC_FAIL) return 0;
+  *bit = best;
+  return 1;
+}
+
+/* Sync start inside the dynamic block whose header is at table_bit: the
+ * positions of its code walked from ORC_SYNC_OFFSETS start bits of
+ * [from, to) to the first symbol boundary >= from + offsets + span; an EOB
+ * or an invalid code ends a walk as failed. */
+int orc_dyn_sync_find(const uint8_t *data, size_t n, uint64_t table_bit, uint64_t from,
+                      uint64_t to, uint64_t *bit) {
+  const uint64_t target = from + ORC_SYNC_OFFSETS + ORC_SYNC_SPAN_DYN;
+  if (target + 64 > to || target + 128 > (uint64_t)n * 8) return 0;
+  br_t hb = {data, n, table_bit};
+  if ((br_read(&hb, 3) >> 1) != 2) return 0;
+  htab_t *t = (htab_t *)malloc(2 * sizeof(htab_t));
+  if (read_dynamic(&hb, &t[0], &t[1])) {
+    free(t);
+    return 0;
+  }
+  uint64_t e[ORC_SYNC_OFFSETS];
+  for (int i = 0; i < ORC_SYNC_OFFSETS; i++) {
+    br_t b = {data, n, from + i};
+    e[i] = SYNC_FAIL;
+    while (b.pos < target) {
+      int sym = htab_decode(&t[0], &b);
+      if (sym < 0 || sym == 256 || sym > 285) break;
+      if (sym > 256) {
+        b.pos += LEN_EXTRA[sym - 257];
+        int ds = htab_decode(&t[1], &b);
+        if (ds < 0 || ds >= 30) break;
+        b.pos += DIST_EXTRA[ds];
+      }
+      if (b.pos >= target) e[i] = b.pos;
+    }
+  }
+  free(t);
   uint64_t best = SYNC_FAIL;
   int best_n = 1;
   for (int i = 0; i < ORC_SYNC_OFFSETS; i++) {

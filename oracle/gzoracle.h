@@ -35,11 +35,13 @@ enum {
 
 /* flags of orc_inflate_chunk_ex */
 enum {
-  ORC_START_FIXED = 1, /* start inside a non-final fixed-Huffman block (a sync start) */
+  ORC_START_SYNC = 1,  /* a sync start: inside the block whose header is at start_table
+                          (0: a non-final fixed-Huffman block) */
   ORC_ZERO_WINDOW = 2, /* back-references before the chunk read zeros (member start) */
 };
 #define ORC_SYNC_OFFSETS 64
 #define ORC_SYNC_SPAN 8192
+#define ORC_SYNC_SPAN_DYN 16384
 
 /* window modes for orc_inflate_chunk */
 enum {
@@ -98,11 +100,17 @@ int orc_inflate_chunk(const uint8_t *data, size_t n, uint64_t start_bit, uint64_
 
 /* code lengths of the dynamic block header at `bit` (litlen then dist) */
 /* orc_inflate_chunk with sync-start modes (no reference counterpart; the
- * device decoder's sync starts in fixed-Huffman data): see gzoracle.c
- * inflate_core.  *sync_end = 1 when the chunk stopped at a sync target. */
+ * device decoder's sync starts): see gzoracle.c inflate_core.  *sync_end =
+ * 1 when the chunk stopped at a sync target; *end_hdr = the header bit of
+ * the block it stopped in (0 for a fixed sync start). */
 int orc_inflate_chunk_ex(const uint8_t *data, size_t n, uint64_t start_bit, uint64_t stop_lo,
-                         int flags, const uint64_t *sync_targets, size_t n_targets,
-                         uint16_t *out, size_t cap, orc_chunk_result *res, uint32_t *sync_end);
+                         int flags, uint64_t start_table, const uint64_t *sync_targets,
+                         const uint64_t *target_tables, size_t n_targets, uint16_t *out,
+                         size_t cap, orc_chunk_result *res, uint32_t *sync_end,
+                         uint64_t *end_hdr);
+/* Sync start inside the dynamic block whose header is at table_bit. */
+int orc_dyn_sync_find(const uint8_t *data, size_t n, uint64_t table_bit, uint64_t from,
+                      uint64_t to, uint64_t *bit);
 /* Sync start in fixed-Huffman data for the range [from, to): 1 and *bit, or 0. */
 int orc_fixed_sync_find(const uint8_t *data, size_t n, uint64_t from, uint64_t to, uint64_t *bit);
 int orc_dynamic_lengths(const uint8_t *data, size_t n, uint64_t bit, uint8_t *lens, int *nlen,

@@ -73,10 +73,12 @@ def lib():
             L.orc_is_dynamic_candidate.argtypes = [vp, sz, u64]
             L.orc_inflate_chunk.argtypes = [vp, sz, u64, u64, ctypes.c_int, vp, sz, vp, sz,
                                             ctypes.POINTER(ChunkResult)]
-            L.orc_inflate_chunk_ex.argtypes = [vp, sz, u64, u64, ctypes.c_int, vp, sz, vp, sz,
-                                               ctypes.POINTER(ChunkResult),
-                                               ctypes.POINTER(ctypes.c_uint32)]
+            L.orc_inflate_chunk_ex.argtypes = [vp, sz, u64, u64, ctypes.c_int, u64, vp, vp, sz, vp,
+                                               sz, ctypes.POINTER(ChunkResult),
+                                               ctypes.POINTER(ctypes.c_uint32),
+                                               ctypes.POINTER(u64)]
             L.orc_fixed_sync_find.argtypes = [vp, sz, u64, u64, ctypes.POINTER(u64)]
+            L.orc_dyn_sync_find.argtypes = [vp, sz, u64, u64, u64, ctypes.POINTER(u64)]
             L.orc_dynamic_lengths.argtypes = [vp, sz, u64, vp, ctypes.POINTER(ctypes.c_int),
                                               ctypes.POINTER(ctypes.c_int)]
             L.orc_scan_members.argtypes = [vp, sz, vp, sz]
@@ -144,24 +146,39 @@ def inflate_chunk(data, start_bit: int, stop_lo: int = 2**64 - 1, window=None,
     return st, res, out[:res.out_len].copy()
 
 
-START_FIXED, ZERO_WINDOW = 1, 2
+START_SYNC, ZERO_WINDOW = 1, 2
 
 
 def inflate_chunk_ex(data, start_bit: int, stop_lo: int = 2**64 - 1, flags: int = 0,
-                     sync_targets=(), cap: int | None = None):
-    """orc_inflate_chunk_ex: a chunk that may start inside a fixed-Huffman
-    block (START_FIXED) and stop at its successors' sync starts.  Returns
-    (status, ChunkResult, u16 entries, sync_end)."""
+                     start_table: int = 0, sync_targets=(), target_tables=None,
+                     cap: int | None = None):
+    """orc_inflate_chunk_ex: a chunk that may be a sync start (START_SYNC,
+    inside the block whose header is at start_table; 0 = a fixed block) and
+    stop at its successors' sync starts (target_tables: each one's block
+    header, 0 = fixed).  Returns (status, ChunkResult, u16 entries, sync_end,
+    end_hdr)."""
     a = _u8(data)
     cap = cap or max(1 << 16, a.size * 16)
     out = np.zeros(cap, np.uint16)
     res = ChunkResult()
     t = np.ascontiguousarray(sync_targets, dtype=np.uint64)
+    tt = np.ascontiguousarray(target_tables if target_tables is not None else np.zeros(t.size),
+                              dtype=np.uint64)
     se = ctypes.c_uint32(0)
-    st = lib().orc_inflate_chunk_ex(a.ctypes.data, a.size, start_bit, stop_lo, flags,
-                                    t.ctypes.data if t.size else None, t.size, out.ctypes.data,
-                                    cap, ctypes.byref(res), ctypes.byref(se))
-    return st, res, out[:res.out_len].copy(), int(se.value)
+    eh = ctypes.c_uint64(0)
+    st = lib().orc_inflate_chunk_ex(a.ctypes.data, a.size, start_bit, stop_lo, flags, start_table,
+                                    t.ctypes.data if t.size else None,
+                                    tt.ctypes.data if t.size else None, t.size, out.ctypes.data,
+                                    cap, ctypes.byref(res), ctypes.byref(se), ctypes.byref(eh))
+    return st, res, out[:res.out_len].copy(), int(se.value), int(eh.value)
+
+
+def dyn_sync_find(data, table_bit: int, from_bit: int, to_bit: int):
+    """Sync start in the dynamic block whose header is at table_bit, or None."""
+    a = _u8(data)
+    b = ctypes.c_uint64(0)
+    ok = lib().orc_dyn_sync_find(a.ctypes.data, a.size, table_bit, from_bit, to_bit, ctypes.byref(b))
+    return int(b.value) if ok else None
 
 
 def fixed_sync_find(data, from_bit: int, to_bit: int):

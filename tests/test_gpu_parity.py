@@ -360,8 +360,8 @@ def test_sync_chunks_match_oracle(G, ctx):
     n_synced = 0
     for i, (s, stop, fl) in enumerate(chunks):
         targets = starts[i:i + 5]                             # successors: all sync starts
-        st, r, e, se = O.inflate_chunk_ex(c, s, stop, flags=(O.START_FIXED if fl & 2 else O.ZERO_WINDOW),
-                                          sync_targets=targets, cap=cap)
+        st, r, e, se, _ = O.inflate_chunk_ex(c, s, stop, flags=(O.START_SYNC if fl & 2 else O.ZERO_WINDOW),
+                                             sync_targets=targets, cap=cap)
         assert int(res[i, 4]) == st, i
         if st != O.OK:
             continue
@@ -385,3 +385,83 @@ def test_level1_fixed_streams_split(G):
         assert int(((d["flags"] & 8) != 0).sum()) >= 4
         assert int(r["sync_end"].sum()) >= 4
         cx.close()
+
+
+def _first_block(c):
+    _, hl = O.gzip_header_len(c)
+    h = hl * 8
+    st, r, _ = O.inflate_chunk(c, h, stop_lo=h + 1, cap=16 << 20)
+    assert st == O.OK
+    return h, r.end_bit
+
+
+def test_dyn_sync_find_matches_oracle(ctx):
+    """Sync starts inside a dynamic block equal the oracle's."""
+    for ctype, seed in ((W.RUNS, 51), (W.MARKOV, 52), (W.RAMPS, 53)):
+        p, c = _stream(ctype, 6, 3 << 20, seed=seed)
+        h, end = _first_block(c)
+        items = [(h, g, g + 40000) for g in range(h + 3000, end - 40000, 17000)]
+        got = ctx.debug_dyn_sync(c, items)
+        exp = [O.dyn_sync_find(c, t, f, e) for t, f, e in items]
+        assert got == exp, (ctype, got, exp)
+        if ctype != W.RAMPS:
+            assert sum(x is not None for x in got) >= len(items) // 2
+
+
+def test_dyn_sync_chunks_match_oracle(ctx):
+    """A dynamic block cut at sync starts: entries, end bits, sync ends and
+    end headers equal the oracle's, and a bogus sync start is gone by."""
+    p, c = _stream(W.RUNS, 6, 3 << 20, seed=54)
+    h, end = _first_block(c)
+    syncs = [O.dyn_sync_find(c, h, g, g + 40000) for g in range(h + 3000, end - 40000, 40000)]
+    syncs = [b for b in syncs if b is not None][:4]
+    assert len(syncs) >= 3
+    starts = [syncs[0], syncs[1] + 1, syncs[1]] + syncs[2:]
+    starts = sorted(set(starts))
+    chunks = [(h, starts[0], 1)] + [(s, starts[k + 1] if k + 1 < len(starts) else 2**64 - 1, 2)
+                                     for k, s in enumerate(starts)]
+    tables = [0] + [h] * len(starts)
+    cap = 8 << 20
+    res, ent = ctx.debug_decode(c, chunks, cap, tables=tables)
+    n_synced = 0
+    for i, (s, stop, fl) in enumerate(chunks):
+        tg = starts[i:i + 5]
+        st, r, e, se, eh = O.inflate_chunk_ex(
+            c, s, stop, flags=(O.START_SYNC if fl & 2 else O.ZERO_WINDOW),
+            start_table=(h if fl & 2 else 0), sync_targets=tg, target_tables=[h] * len(tg), cap=cap)
+        assert int(res[i, 4]) == st, i
+        if st != O.OK:
+            continue
+        assert int(res[i, 0]) == r.end_bit and int(res[i, 1]) == r.out_len, i
+        assert int(res[i, 2]) == r.marker_end and int(res[i, 5]) == r.final_block, i
+        assert int(res[i, 3]) == r.n_blocks and int(res[i, 6]) == se, i
+        assert np.array_equal(ent[i, :r.out_len], e), i
+        n_synced += se
+    assert n_synced >= 2
+
+
+def test_high_ratio_partitions_split_at_dyn_sync(G):
+    """Byte runs (about 15x): partitions are cut by their output estimate and
+    the pieces start at sync starts inside dynamic blocks; byte-exact."""
+    p, c = _stream(W.RUNS, 6, 24 << 20, seed=55)
+    cx = G.Context(chunk_bytes=64 << 10)
+    assert cx.decompress(c) == p.tobytes()
+    d, r = cx.last_chunks()
+    dyn = ((d["flags"] & 8) != 0) & (d["table_bit"] != 0)
+    assert int(dyn.sum()) >= 4
+    assert int((r["sync_end"][:len(d)] != 0).sum()) >= 4
+    cx.close()
+
+
+def test_sync_start_naming_a_fixed_block_header(ctx):
+    """A sync start may name its block's header when that block is fixed (a
+    repair after a mid-block handover does): same entries as the oracle."""
+    p, c = _level1(W.MARKOV, 1 << 20, 56)
+    h, end = _first_block(c)
+    b = O.fixed_sync_find(c, h + 2000, end)
+    assert b is not None
+    res, ent = ctx.debug_decode(c, [(b, 2**64 - 1, 2)], 4 << 20, tables=[h])
+    st, r, e, se, _ = O.inflate_chunk_ex(c, b, flags=O.START_SYNC, start_table=h, cap=4 << 20)
+    assert st == O.OK and int(res[0, 4]) == st
+    assert int(res[0, 0]) == r.end_bit and int(res[0, 1]) == r.out_len
+    assert np.array_equal(ent[0, :r.out_len], e)
