@@ -529,6 +529,23 @@ def cpu_baseline(comp: np.ndarray, meta: dict, budget_s: float = 12.0, threads: 
                       f"(oracle chunked decoder, 4 MiB chunks, median)"}
 
 
+def max_over_ranks(ms: float, dist, device: str = "cuda") -> float:
+    """The job's time: the slowest rank's (all ranks take part; every rank
+    gets the result).  `dist` is None for one process."""
+    if dist is None:
+        return ms
+    import torch
+    t = torch.tensor([ms], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_gbs(world: int, steps: int, bytes_per_step: int, ms: float) -> float:
+    """Whole-job decompressed GB/s: every rank decodes its own replica
+    (weak scaling), so the job moves world x steps x bytes in `ms`."""
+    return world * steps * bytes_per_step / (ms / 1e3) / 1e9
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -650,12 +667,8 @@ def main():
         e1.record()
         torch.cuda.synchronize()
         barrier()
-    ms = e0.elapsed_time(e1)
-    if dist is not None:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = world * args.steps * meta["plain_bytes"] / (ms / 1e3) / 1e9
+    ms = max_over_ranks(e0.elapsed_time(e1), dist)
+    value = job_gbs(world, args.steps, meta["plain_bytes"], ms)
     clocks = clk.summary()
 
     # ---- e2e through the host C-ABI call with pinned buffers -------------------
@@ -675,13 +688,9 @@ def main():
     f1.record()
     torch.cuda.synchronize()
     barrier()
-    e2e_ms = f0.elapsed_time(f1)
-    if dist is not None:
-        t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(f0.elapsed_time(f1), dist)
     e2e_ok = hashlib.sha256(hout_np[:n].tobytes()).hexdigest() == meta["sha256"]
-    e2e = {"value": round(world * e2e_steps * meta["plain_bytes"] / (e2e_ms / 1e3) / 1e9, 4),
+    e2e = {"value": round(job_gbs(world, e2e_steps, meta["plain_bytes"], e2e_ms), 4),
            "unit": "GB/s", "h2d_bytes_per_step": int(comp.size),
            "d2h_bytes_per_step": int(meta["plain_bytes"]), "byte_exact": bool(e2e_ok)}
 

@@ -165,6 +165,7 @@ struct gzgpu_ctx {
   bool autotune = false;
   bool ring = false;  // history layout of the inflate kernel (false = pages)
   int ctas_per_sm = 3;  // page kernel CTAs per SM (3 or 4)
+  bool fine_split = false;  // output-estimate pieces + dynamic-block sync starts
   int decode_blocks = 0;
   cudaEvent_t ev[12];
   gzgpu_stats stats{};
@@ -511,7 +512,7 @@ int gzgpu_ctx::run(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R) 
   // dynamic start's output per input byte from its code lengths.  Partitions
   // expected to produce more than twice 2 x chunk_bytes are cut into pieces
   // of about that output, which get their own finder pass.
-  if (!hspec.empty()) {
+  if (fine_split && !hspec.empty()) {
     if ((rc = check(cudaMemcpyAsync(hd.data(), descs.p, sizeof(ChunkDesc) * n_grid,
                                     cudaMemcpyDeviceToHost, st))) ||
         (rc = check(cudaStreamSynchronize(st))))
@@ -1089,6 +1090,7 @@ int gzgpu_create(gzgpu_ctx** out, const gzgpu_config* cfg) {
     c->autotune = cfg->autotune != 0;
     c->ring = cfg->ring_history != 0;
     if (cfg->ctas_per_sm == 3 || cfg->ctas_per_sm == 4) c->ctas_per_sm = cfg->ctas_per_sm;
+    c->fine_split = cfg->fine_split != 0;
   }
   if (cudaSetDevice(c->dev) != cudaSuccess) {
     delete c;

@@ -811,16 +811,16 @@ __device__ int32_t decode_chunk(const uint8_t* __restrict__ in, ChunkDesc d,
   uint32_t bfinal = 0, btype = 0;
   bool resume = false;  // continue the current block after going by a successor
   const bool confirmed = (d.flags & (kChunkMemberFirst | kChunkConfirmed)) != 0;
-  // move on past successor d.next (a phantom)
-  auto extend = [&](const ChunkDesc& nx) {
-    if (nx.next == kNoChunk) {
+  // move on past successor d.next (a phantom) to nx_next, the chunk after it
+  auto extend = [&](uint32_t nx_next) {
+    if (nx_next == kNoChunk) {
       d.stop_lo = kNoStop;
       d.abort_bit = kNoStop;
     } else {
-      d.stop_lo = handover_bit(descs[nx.next]);
+      d.stop_lo = handover_bit(descs[nx_next]);
       if (d.abort_bit != kNoStop) d.abort_bit = d.stop_lo + slack;
     }
-    d.next = nx.next;
+    d.next = nx_next;
     extends++;
     set_limit();
   };
@@ -867,11 +867,10 @@ __device__ int32_t decode_chunk(const uint8_t* __restrict__ in, ChunkDesc d,
     if (resume_now) {
       // successors whose start this chunk is already past, mid-block
       while (d.next != kNoChunk && (confirmed || extends < kMaxExtends)) {
-        const ChunkDesc nx = descs[d.next];
-        if ((nx.flags & kChunkMemberFirst) ||
+        if ((descs[d.next].flags & kChunkMemberFirst) ||
             ((const volatile ChunkDesc*)(descs + d.next))->start_bit >= bitpos)
           break;
-        extend(nx);
+        extend(descs[d.next].next);
       }
     }
     if (bitpos > d.abort_bit) {
@@ -987,7 +986,7 @@ __device__ int32_t decode_chunk(const uint8_t* __restrict__ in, ChunkDesc d,
                                          passed, lane);
         if (status != kOk || synced) break;
         if (passed) {
-          extend(descs[d.next]);
+          extend(descs[d.next].next);
           resume = true;
           continue;
         }

@@ -62,6 +62,11 @@ typedef struct {
                          of the output pages in HBM (32 warps/SM, the default) */
   int ctas_per_sm;    /* page-history decoder: 3 (24 warps/SM, 80 registers; default) or
                          4 (32 warps/SM, 64 registers); 0 = default */
+  int fine_split;     /* 1 = cut partitions whose first blocks promise a high output
+                         ratio into pieces and give pieces without a block start a
+                         sync start inside their dynamic block; 0 = off (default:
+                         measured no faster on the mixed, multi-member and batch
+                         workloads) */
 } gzgpu_config;
 
 typedef struct {

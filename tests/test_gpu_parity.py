@@ -441,10 +441,11 @@ def test_dyn_sync_chunks_match_oracle(ctx):
 
 
 def test_high_ratio_partitions_split_at_dyn_sync(G):
-    """Byte runs (about 15x): partitions are cut by their output estimate and
-    the pieces start at sync starts inside dynamic blocks; byte-exact."""
+    """Byte runs (about 15x) with fine_split: partitions are cut by their
+    output estimate and the pieces start at sync starts inside dynamic
+    blocks; byte-exact."""
     p, c = _stream(W.RUNS, 6, 24 << 20, seed=55)
-    cx = G.Context(chunk_bytes=64 << 10)
+    cx = G.Context(chunk_bytes=64 << 10, fine_split=True)
     assert cx.decompress(c) == p.tobytes()
     d, r = cx.last_chunks()
     dyn = ((d["flags"] & 8) != 0) & (d["table_bit"] != 0)
