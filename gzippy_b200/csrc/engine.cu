@@ -166,6 +166,7 @@ struct gzgpu_ctx {
   bool ring = false;  // history layout of the inflate kernel (false = pages)
   int ctas_per_sm = 3;  // page kernel CTAs per SM (3 or 4)
   bool fine_split = false;  // output-estimate pieces + dynamic-block sync starts
+  bool job_sync = true;     // the running job has sync starts (decoder variant)
   int decode_blocks = 0;
   cudaEvent_t ev[12];
   gzgpu_stats stats{};
@@ -203,15 +204,15 @@ struct gzgpu_ctx {
     stats.decode_passes++;
     switch (lut_bits) {
       case 11:
-        return launch_inflate<11>(ring, ctas_per_sm, cur_in, descs.as<ChunkDesc>(), results.as<ChunkResult>(),
+        return launch_inflate<11>(ring, ctas_per_sm, job_sync, cur_in, descs.as<ChunkDesc>(), results.as<ChunkResult>(),
                                   work.as<uint32_t>(), d_work_count, counters.as<uint32_t>() + 3,
                                   pool, decode_blocks, st);
       case 12:
-        return launch_inflate<12>(ring, ctas_per_sm, cur_in, descs.as<ChunkDesc>(), results.as<ChunkResult>(),
+        return launch_inflate<12>(ring, ctas_per_sm, job_sync, cur_in, descs.as<ChunkDesc>(), results.as<ChunkResult>(),
                                   work.as<uint32_t>(), d_work_count, counters.as<uint32_t>() + 3,
                                   pool, decode_blocks, st);
       default:
-        return launch_inflate<10>(ring, ctas_per_sm, cur_in, descs.as<ChunkDesc>(), results.as<ChunkResult>(),
+        return launch_inflate<10>(ring, ctas_per_sm, job_sync, cur_in, descs.as<ChunkDesc>(), results.as<ChunkResult>(),
                                   work.as<uint32_t>(), d_work_count, counters.as<uint32_t>() + 3,
                                   pool, decode_blocks, st);
     }
@@ -503,8 +504,9 @@ int gzgpu_ctx::run(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R) 
   cudaMemsetAsync(counters.as<uint32_t>() + 1, 0, 4, st);
   cudaEventRecord(ev[3], st);
   // ---- 3. finder + link ---------------------------------------------------
+  uint32_t* n_sync = counters.as<uint32_t>() + 4;  // sync starts found (zeroed with the scan)
   if ((rc = check(launch_finder(cur_in, descs.as<ChunkDesc>(), spec.as<uint32_t>(),
-                                (uint32_t)hspec.size(), st))))
+                                (uint32_t)hspec.size(), n_sync, st))))
     return rc;
   stats.kernel_launches += 2;
   // ---- 3a. cut high-ratio partitions finer ---------------------------------
@@ -571,7 +573,7 @@ int gzgpu_ctx::run(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R) 
       cudaMemcpyAsync(descs.p, hd.data(), sizeof(ChunkDesc) * n_grid, cudaMemcpyHostToDevice, st);
       cudaMemcpyAsync(spec.p, hspec2.data(), 4 * hspec2.size(), cudaMemcpyHostToDevice, st);
       if ((rc = check(launch_finder(cur_in, descs.as<ChunkDesc>(), spec.as<uint32_t>(),
-                                    (uint32_t)hspec2.size(), st))))
+                                    (uint32_t)hspec2.size(), n_sync, st))))
         return rc;
       stats.kernel_launches += 2;
     }
@@ -584,7 +586,7 @@ int gzgpu_ctx::run(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R) 
       if ((rc = check(spec.ensure(4 * (hsync.size() + 1))))) return rc;
       cudaMemcpyAsync(spec.p, hsync.data(), 4 * hsync.size(), cudaMemcpyHostToDevice, st);
       if ((rc = check(launch_dyn_sync(cur_in, descs.as<ChunkDesc>(), spec.as<uint32_t>(),
-                                      (uint32_t)hsync.size(), st))))
+                                      (uint32_t)hsync.size(), n_sync, st))))
         return rc;
       stats.kernel_launches += 1;
     }
@@ -595,6 +597,14 @@ int gzgpu_ctx::run(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R) 
                               st))))
     return rc;
   stats.kernel_launches += 1;
+  {
+    // the decoder variant without sync-start handling when there are none
+    uint32_t h_sync = 1;
+    if ((rc = check(cudaMemcpyAsync(&h_sync, n_sync, 4, cudaMemcpyDeviceToHost, st))) ||
+        (rc = check(cudaStreamSynchronize(st))))
+      return rc;
+    job_sync = h_sync != 0;
+  }
   cudaEventRecord(ev[4], st);
   // ---- 4. decode ----------------------------------------------------------
   uint64_t pages_needed = (est_out + n_grid * (uint64_t)kPageEntries) / kPageEntries + 64;
@@ -1504,7 +1514,7 @@ int gzgpu_debug_find(gzgpu_ctx* c, const uint8_t* in, size_t in_len, const uint6
     cudaMemcpyAsync(c->descs.p, d.data(), sizeof(ChunkDesc) * n, cudaMemcpyHostToDevice, c->st);
     cudaMemcpyAsync(c->spec.p, sp.data(), 4 * n, cudaMemcpyHostToDevice, c->st);
     if ((rc = c->check(launch_finder(c->in.as<uint8_t>(), c->descs.as<ChunkDesc>(),
-                                     c->spec.as<uint32_t>(), (uint32_t)n, c->st))))
+                                     c->spec.as<uint32_t>(), (uint32_t)n, nullptr, c->st))))
       return rc;
     cudaMemcpyAsync(d.data(), c->descs.p, sizeof(ChunkDesc) * n, cudaMemcpyDeviceToHost, c->st);
   }
@@ -1553,7 +1563,7 @@ int gzgpu_debug_dyn_sync(gzgpu_ctx* c, const uint8_t* in, size_t in_len, const u
     cudaMemcpyAsync(c->descs.p, d.data(), sizeof(ChunkDesc) * 2 * n, cudaMemcpyHostToDevice, c->st);
     cudaMemcpyAsync(c->spec.p, pieces.data(), 4 * n, cudaMemcpyHostToDevice, c->st);
     if ((rc = c->check(launch_dyn_sync(c->in.as<uint8_t>(), c->descs.as<ChunkDesc>(),
-                                       c->spec.as<uint32_t>(), (uint32_t)n, c->st))))
+                                       c->spec.as<uint32_t>(), (uint32_t)n, nullptr, c->st))))
       return rc;
     cudaMemcpyAsync(d.data(), c->descs.p, sizeof(ChunkDesc) * 2 * n, cudaMemcpyDeviceToHost, c->st);
   }
@@ -1610,6 +1620,8 @@ int gzgpu_debug_decode(gzgpu_ctx* c, const uint8_t* in, size_t in_len, const uin
   }
   cudaMemcpyAsync(c->counters.as<uint32_t>() + 1, &nn, 4, cudaMemcpyHostToDevice, c->st);
   c->cur_in = c->in.as<uint8_t>();
+  c->job_sync = false;
+  for (size_t i = 0; i < n; i++) c->job_sync |= (d[i].flags & kChunkSync) != 0;
   if ((rc = c->check(c->launch_decode(c->counters.as<uint32_t>() + 1)))) return rc;
   std::vector<ChunkResult> r(n);
   uint32_t used = 0;

@@ -77,7 +77,7 @@ __global__ void __launch_bounds__(32 * kFinderWarps)
 // and the input.
 __global__ void __launch_bounds__(kSyncOffsets)
     sync_kernel(const uint8_t* __restrict__ in, ChunkDesc* descs, const uint32_t* __restrict__ spec,
-                uint32_t n_spec) {
+                uint32_t n_spec, uint32_t* n_sync) {
   __shared__ uint32_t sync_words[kSyncWords];
   __shared__ uint64_t sync_end[kSyncOffsets];
   if (blockIdx.x >= n_spec) return;
@@ -109,6 +109,7 @@ __global__ void __launch_bounds__(kSyncOffsets)
     if (best != kSyncFail) {
       d.lo_bit = d.start_bit = best;
       d.flags |= kChunkValid | kChunkSync;
+      if (n_sync) atomicAdd(n_sync, 1u);
     }
   }
 }
@@ -157,10 +158,10 @@ __global__ void link_kernel(ChunkDesc* descs, uint32_t n, uint32_t* work, uint32
 }
 
 cudaError_t launch_finder(const uint8_t* in, ChunkDesc* descs, const uint32_t* spec,
-                          uint32_t n_spec, cudaStream_t stream) {
+                          uint32_t n_spec, uint32_t* n_sync, cudaStream_t stream) {
   if (n_spec == 0) return cudaSuccess;
   finder_kernel<<<n_spec, 32 * kFinderWarps, 0, stream>>>(in, descs, spec, n_spec);
-  sync_kernel<<<n_spec, kSyncOffsets, 0, stream>>>(in, descs, spec, n_spec);
+  sync_kernel<<<n_spec, kSyncOffsets, 0, stream>>>(in, descs, spec, n_spec, n_sync);
   return cudaGetLastError();
 }
 

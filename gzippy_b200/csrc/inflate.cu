@@ -531,7 +531,9 @@ __device__ __forceinline__ uint16_t* page_addr(const PageHist& ph, int32_t rel) 
   return ph.data + (size_t)pg * kPageEntries + ((uint32_t)rel & (kPageEntries - 1));
 }
 
-template <int LB>
+// kSync: the successor checks for sync starts and for starts gone by
+// mid-block (compiled out when the job has no sync starts)
+template <int LB, bool kSync>
 __device__ int32_t huff_block_parallel(BitReader& br, const Tables<LB>* T, PageHist& ph,
                                        const PagePool& pool, uint32_t cid, uint32_t gen,
                                        uint64_t& o, uint64_t& guard, uint64_t& marker_end,
@@ -545,7 +547,7 @@ __device__ int32_t huff_block_parallel(BitReader& br, const Tables<LB>* T, PageH
     // the successor's sync start: stop exactly there if it is a symbol
     // start of this block; rt = its offset in this step (>= 32: not here)
     uint32_t rt = 1000;
-    if (sync_target != kNoStop && sync_target >= pos) {
+    if (kSync && sync_target != kNoStop && sync_target >= pos) {
       if (sync_target == pos) {
         synced = true;
         break;
@@ -621,7 +623,7 @@ __device__ int32_t huff_block_parallel(BitReader& br, const Tables<LB>* T, PageH
     // (chain positions stay below 32 + 48)
     const uint32_t kind0 = (info >> 6) & 3;
     uint32_t nxt = ((info & 0x100) || kind0 >= kKindEob) ? 128u + lane : lane + (info & 63);
-    if (nxt == rt) nxt = 96;  // the walk ends at the sync start
+    if (kSync && nxt == rt) nxt = 96;  // the walk ends at the sync start
     // walk the chain of symbols that start in bits [0, 32)
     uint32_t path = 0, p = 0;
     bool eob = false;
@@ -659,14 +661,14 @@ __device__ int32_t huff_block_parallel(BitReader& br, const Tables<LB>* T, PageH
           eob = true;
           break;
         }
-        if (p == rt) p = 96;
+        if (kSync && p == rt) p = 96;
         continue;
       }
       path |= 1u << p;
       p = __shfl_sync(0xFFFFFFFFu, nxt, p & 31);
     }
     if (status != kOk) break;
-    const bool at_sync = p == 96;
+    const bool at_sync = kSync && p == 96;
     if (at_sync) p = rt;
     // output offsets: exclusive prefix sum of output lengths along the chain
     const bool on = (path >> lane) & 1;
@@ -734,7 +736,7 @@ __device__ int32_t huff_block_parallel(BitReader& br, const Tables<LB>* T, PageH
     }
     if (eob) break;
     // the successor's start went by mid-block: it can never be handed over
-    if (passed_bit < pos) {
+    if (kSync && passed_bit < pos) {
       passed = true;
       break;
     }
@@ -752,7 +754,7 @@ __device__ __forceinline__ uint64_t handover_bit(const ChunkDesc& k) {
   return (k.flags & kChunkMemberFirst) ? k.limit_bit * 8 : k.lo_bit;
 }
 
-template <int LB, bool kRing>
+template <int LB, bool kRing, bool kSync>
 __device__ int32_t decode_chunk(const uint8_t* __restrict__ in, ChunkDesc d,
                                 const ChunkDesc* descs, ChunkResult* res, uint32_t cid,
                                 uint32_t gen, uint16_t* ring, Tables<LB>* T,
@@ -805,7 +807,7 @@ __device__ int32_t decode_chunk(const uint8_t* __restrict__ in, ChunkDesc d,
   const uint64_t slack = d.abort_bit != kNoStop ? d.abort_bit - d.stop_lo : 0;
   // a sync start begins inside a block: the Huffman block whose header is at
   // d.table_bit, or (table_bit 0) a non-final fixed-Huffman block
-  bool in_sync_block = (d.flags & kChunkSync) != 0;
+  bool in_sync_block = kSync && (d.flags & kChunkSync) != 0;
   bool synced = false;
   uint64_t blk_hdr = 0;  // header bit of the block being decoded (0 = unknown)
   uint32_t bfinal = 0, btype = 0;
@@ -970,7 +972,7 @@ __device__ int32_t decode_chunk(const uint8_t* __restrict__ in, ChunkDesc d,
         // goes by mid-block is a phantom (real starts are block boundaries
         // or sync starts reached exactly): the decode moves on past it.
         uint64_t sync_target = kNoStop, passed_bit = kNoStop;
-        if (d.next != kNoChunk) {
+        if (kSync && d.next != kNoChunk) {
           const ChunkDesc& nx = descs[d.next];
           if (nx.flags & kChunkSync) {
             const bool same = nx.table_bit ? (blk_hdr == nx.table_bit)
@@ -981,7 +983,7 @@ __device__ int32_t decode_chunk(const uint8_t* __restrict__ in, ChunkDesc d,
             passed_bit = ((const volatile ChunkDesc*)(descs + d.next))->start_bit;
         }
         bool passed = false;
-        status = huff_block_parallel<LB>(br, T, ph, pool, cid, gen, o, guard, marker_end,
+        status = huff_block_parallel<LB, kSync>(br, T, ph, pool, cid, gen, o, guard, marker_end,
                                          zero_window, trunc_words, sync_target, passed_bit, synced,
                                          passed, lane);
         if (status != kOk || synced) break;
@@ -1153,7 +1155,7 @@ __device__ int32_t decode_chunk(const uint8_t* __restrict__ in, ChunkDesc d,
 
 // Work loop shared by both kernels: take chunks from the queue; a failed
 // speculative start moves on to the next candidate of its partition.
-template <int LB, bool kRing>
+template <int LB, bool kRing, bool kSync>
 __device__ __forceinline__ void work_loop(const uint8_t* __restrict__ in, ChunkDesc* descs,
                                           ChunkResult* results, const uint32_t* work,
                                           uint32_t n_work, uint32_t* work_counter,
@@ -1171,7 +1173,7 @@ __device__ __forceinline__ void work_loop(const uint8_t* __restrict__ in, ChunkD
     const bool speculative =
         !(d.flags & (kChunkMemberFirst | kChunkSync)) && d.limit_bit > d.lo_bit;
     for (uint32_t gen = 0;; gen++) {
-      int32_t st = decode_chunk<LB, kRing>(in, d, descs, &results[cid], cid, gen, ring, T, pool,
+      int32_t st = decode_chunk<LB, kRing, kSync>(in, d, descs, &results[cid], cid, gen, ring, T, pool,
                                            lane);
       if (st == kOk || st == kPoolExhausted || !speculative || gen + 1 >= kMaxTries) break;
       uint64_t lo = 0, hi = 0;
@@ -1202,11 +1204,11 @@ __global__ void __launch_bounds__(32 * kRingWarps)
   extern __shared__ __align__(16) uint8_t smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   RingSmem<LB>* S = reinterpret_cast<RingSmem<LB>*>(smem) + warp;
-  work_loop<LB, true>(in, descs, results, work, *n_work_ptr, work_counter, pool, S->ring, &S->t,
-                      lane);
+  work_loop<LB, true, true>(in, descs, results, work, *n_work_ptr, work_counter, pool, S->ring,
+                            &S->t, lane);
 }
 
-template <int LB, int MINB>
+template <int LB, int MINB, bool kSync>
 __global__ void __launch_bounds__(32 * kPageWarps, MINB)
     inflate_pages_kernel(const uint8_t* __restrict__ in, ChunkDesc* __restrict__ descs,
                          ChunkResult* __restrict__ results, const uint32_t* __restrict__ work,
@@ -1215,8 +1217,8 @@ __global__ void __launch_bounds__(32 * kPageWarps, MINB)
   extern __shared__ __align__(16) uint8_t smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   Tables<LB>* T = reinterpret_cast<Tables<LB>*>(smem) + warp;
-  work_loop<LB, false>(in, descs, results, work, *n_work_ptr, work_counter, pool, nullptr, T,
-                       lane);
+  work_loop<LB, false, kSync>(in, descs, results, work, *n_work_ptr, work_counter, pool, nullptr,
+                              T, lane);
 }
 
 template <int LB>
@@ -1224,14 +1226,19 @@ size_t inflate_smem_bytes(bool ring) {
   return ring ? sizeof(RingSmem<LB>) * kRingWarps : sizeof(Tables<LB>) * kPageWarps;
 }
 
-// page kernel instance for `ctas` CTAs per SM (registers sized for it)
+// page kernel instance for `ctas` CTAs per SM (registers sized for it), with
+// or without sync-start support
 template <int LB>
-static const void* pages_kernel_fn(int ctas) {
-  return ctas >= 4 ? (const void*)inflate_pages_kernel<LB, 4> : (const void*)inflate_pages_kernel<LB, 3>;
+static const void* pages_kernel_fn(int ctas, bool sync) {
+  if (sync)
+    return ctas >= 4 ? (const void*)inflate_pages_kernel<LB, 4, true>
+                     : (const void*)inflate_pages_kernel<LB, 3, true>;
+  return ctas >= 4 ? (const void*)inflate_pages_kernel<LB, 4, false>
+                   : (const void*)inflate_pages_kernel<LB, 3, false>;
 }
 
 template <int LB>
-cudaError_t launch_inflate(bool ring, int ctas, const uint8_t* in, ChunkDesc* descs,
+cudaError_t launch_inflate(bool ring, int ctas, bool sync, const uint8_t* in, ChunkDesc* descs,
                            ChunkResult* results, const uint32_t* work, const uint32_t* n_work,
                            uint32_t* work_counter, const PagePool& pool, int blocks,
                            cudaStream_t stream) {
@@ -1244,15 +1251,13 @@ cudaError_t launch_inflate(bool ring, int ctas, const uint8_t* in, ChunkDesc* de
     inflate_ring_kernel<LB><<<blocks, 32 * kRingWarps, smem, stream>>>(in, descs, results, work,
                                                                        n_work, work_counter, pool);
   } else {
-    const void* fn = pages_kernel_fn<LB>(ctas);
+    const void* fn = pages_kernel_fn<LB>(ctas, sync);
     e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    if (ctas >= 4)
-      inflate_pages_kernel<LB, 4><<<blocks, 32 * kPageWarps, smem, stream>>>(
-          in, descs, results, work, n_work, work_counter, pool);
-    else
-      inflate_pages_kernel<LB, 3><<<blocks, 32 * kPageWarps, smem, stream>>>(
-          in, descs, results, work, n_work, work_counter, pool);
+    void* args[] = {(void*)&in,   (void*)&descs,        (void*)&results, (void*)&work,
+                    (void*)&n_work, (void*)&work_counter, (void*)&pool};
+    e = cudaLaunchKernel(fn, dim3(blocks), dim3(32 * kPageWarps), args, smem, stream);
+    if (e != cudaSuccess) return e;
   }
   return cudaGetLastError();
 }
@@ -1266,9 +1271,12 @@ int inflate_blocks_per_sm(bool ring, int ctas) {
                          (int)smem);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, inflate_ring_kernel<LB>, 32 * kRingWarps, smem);
   } else {
-    const void* fn = pages_kernel_fn<LB>(ctas);
+    // both variants are sized for the same registers; take the larger
+    const void* fn = pages_kernel_fn<LB>(ctas, true);
     cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, 32 * kPageWarps, smem);
+    cudaFuncSetAttribute(pages_kernel_fn<LB>(ctas, false), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)smem);
     if (n > ctas) n = ctas;
   }
   return n;
@@ -1277,7 +1285,7 @@ int inflate_blocks_per_sm(bool ring, int ctas) {
 #define GZGPU_INST(LB)                                                                       \
   template size_t inflate_smem_bytes<LB>(bool);                                              \
   template int inflate_blocks_per_sm<LB>(bool, int);                                         \
-  template cudaError_t launch_inflate<LB>(bool, int, const uint8_t*, ChunkDesc*, ChunkResult*, \
+  template cudaError_t launch_inflate<LB>(bool, int, bool, const uint8_t*, ChunkDesc*, ChunkResult*, \
                                           const uint32_t*, const uint32_t*, uint32_t*,       \
                                           const PagePool&, int, cudaStream_t);
 GZGPU_INST(10)
@@ -1302,7 +1310,7 @@ constexpr uint32_t kSyncScan = 256;  // chunks looked back for a block header
 
 __global__ void __launch_bounds__(kSyncOffsets)
     dyn_sync_kernel(const uint8_t* __restrict__ in, ChunkDesc* descs,
-                    const uint32_t* __restrict__ pieces, uint32_t n) {
+                    const uint32_t* __restrict__ pieces, uint32_t n, uint32_t* n_sync) {
   constexpr int LB = 10;
   __shared__ Tables<LB> T;
   __shared__ uint64_t ends[kSyncOffsets];
@@ -1377,14 +1385,15 @@ __global__ void __launch_bounds__(kSyncOffsets)
       d.lo_bit = d.start_bit = best;
       d.table_bit = table;
       d.flags |= kChunkValid | kChunkSync;
+      if (n_sync) atomicAdd(n_sync, 1u);
     }
   }
 }
 
 cudaError_t launch_dyn_sync(const uint8_t* in, ChunkDesc* descs, const uint32_t* pieces, uint32_t n,
-                            cudaStream_t stream) {
+                            uint32_t* n_sync, cudaStream_t stream) {
   if (!n) return cudaSuccess;
-  dyn_sync_kernel<<<n, kSyncOffsets, 0, stream>>>(in, descs, pieces, n);
+  dyn_sync_kernel<<<n, kSyncOffsets, 0, stream>>>(in, descs, pieces, n, n_sync);
   return cudaGetLastError();
 }
 
@@ -1488,7 +1497,7 @@ __global__ void __launch_bounds__(32)
     if (lane == 0) S->page_next = 0;  // every member starts with an empty pool
     __syncwarp();
     const PagePool pool{S->pages, S->owner, S->seq, &S->page_next, kNoAllocPages};
-    int32_t st = decode_chunk<10, false>(in, d, nullptr, &S->res, 0, 0, nullptr, &T, pool, lane);
+    int32_t st = decode_chunk<10, false, false>(in, d, nullptr, &S->res, 0, 0, nullptr, &T, pool, lane);
     __syncwarp();
     const ChunkResult r = S->res;
     if (st == kPoolExhausted) {

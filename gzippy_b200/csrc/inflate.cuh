@@ -17,12 +17,13 @@ size_t inflate_smem_bytes(bool ring);
 template <int LB>
 int inflate_blocks_per_sm(bool ring, int ctas);
 template <int LB>
-cudaError_t launch_inflate(bool ring, int ctas, const uint8_t* in, ChunkDesc* descs,
+// sync: the job has sync starts (selects the kernel variant that handles them)
+cudaError_t launch_inflate(bool ring, int ctas, bool sync, const uint8_t* in, ChunkDesc* descs,
                            ChunkResult* results, const uint32_t* work, const uint32_t* n_work,
                            uint32_t* work_counter, const PagePool& pool, int blocks,
                            cudaStream_t stream);
 // sync starts inside dynamic blocks for the listed pieces left without a start
 cudaError_t launch_dyn_sync(const uint8_t* in, ChunkDesc* descs, const uint32_t* pieces, uint32_t n,
-                            cudaStream_t stream);
+                            uint32_t* n_sync, cudaStream_t stream);
 
 }  // namespace gzgpu
