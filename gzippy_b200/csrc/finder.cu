@@ -27,8 +27,9 @@ __global__ void __launch_bounds__(32 * kFinderWarps)
   __shared__ uint16_t leaf_lut[4096];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   if (blockIdx.x >= n_spec) return;
-  for (int i = threadIdx.x; i < 4096; i += blockDim.x) leaf_lut[i] = (uint16_t)precode_leaves4(i);
   ChunkDesc& d = descs[spec[blockIdx.x]];
+  if (d.flags & kChunkValid) return;  // a sync start was found first
+  for (int i = threadIdx.x; i < 4096; i += blockDim.x) leaf_lut[i] = (uint16_t)precode_leaves4(i);
   const uint64_t from = d.guess_bit, to = d.limit_bit, nbytes = d.in_end;
   if (threadIdx.x == 0) best_win = ~0ull;
   if (lane == 0) hit_win[warp] = ~0ull;
@@ -71,10 +72,10 @@ __global__ void __launch_bounds__(32 * kFinderWarps)
   }
 }
 
-// Chunks the finder left without a start: look for a sync start in
-// fixed-Huffman data (finder_core.cuh fixed_walk).  One CTA of kSyncOffsets
-// threads per speculative chunk; the walk must end inside the chunk's range
-// and the input.
+// Sync starts in fixed-Huffman data (finder_core.cuh fixed_walk), searched
+// for every speculative chunk before the block finder, which then skips the
+// chunks that have one.  One CTA of kSyncOffsets threads per chunk; the walk
+// must end inside the chunk's range and the input.
 __global__ void __launch_bounds__(kSyncOffsets)
     sync_kernel(const uint8_t* __restrict__ in, ChunkDesc* descs, const uint32_t* __restrict__ spec,
                 uint32_t n_spec, uint32_t* n_sync) {
@@ -160,8 +161,11 @@ __global__ void link_kernel(ChunkDesc* descs, uint32_t n, uint32_t* work, uint32
 cudaError_t launch_finder(const uint8_t* in, ChunkDesc* descs, const uint32_t* spec,
                           uint32_t n_spec, uint32_t* n_sync, cudaStream_t stream) {
   if (n_spec == 0) return cudaSuccess;
-  finder_kernel<<<n_spec, 32 * kFinderWarps, 0, stream>>>(in, descs, spec, n_spec);
+  // The fixed-code sync search first: it costs a fraction of a full scan,
+  // which a fixed-Huffman partition (no block header to find) would need,
+  // and it fails within a few dozen symbols on other data.
   sync_kernel<<<n_spec, kSyncOffsets, 0, stream>>>(in, descs, spec, n_spec, n_sync);
+  finder_kernel<<<n_spec, 32 * kFinderWarps, 0, stream>>>(in, descs, spec, n_spec);
   return cudaGetLastError();
 }
 

@@ -44,6 +44,16 @@ def test_stream_matches_oracle_and_zlib(ctx, ctype, level):
     assert got == ref.tobytes() == p.tobytes() == zlib.decompress(c.tobytes(), 31)
 
 
+def _expected_start(data, f, t):
+    """A partition's start: a sync start in fixed-Huffman data when there is
+    one (searched first), else the first block-start candidate."""
+    b = O.fixed_sync_find(data, f, t)
+    if b is not None:
+        return ("sync", b)
+    first, seek = O.find_blocks(data, f, t, cap=1 << 18)
+    return (int(first[0]), int(seek[0])) if first.size else None
+
+
 def test_finder_matches_oracle(ctx):
     p, c = _stream(W.MARKOV, 6, 2 << 20, seed=3)
     p2, c2 = _stream(W.RANDOM, 6, 1 << 20, seed=4)
@@ -52,8 +62,7 @@ def test_finder_matches_oracle(ctx):
         ranges = [(f, min(f + 64 * 1024 * 8, nbits)) for f in range(80, nbits, 97 * 1024 * 8 + 13)]
         got = ctx.debug_find(data, ranges)
         for (f, t), g in zip(ranges, got):
-            first, seek = O.find_blocks(data, f, t, cap=1 << 18)
-            exp = (int(first[0]), int(seek[0])) if first.size else None
+            exp = _expected_start(data, f, t)
             assert g == exp, (f, t, g, exp)
 
 
@@ -320,8 +329,8 @@ def _level1(ctype, n, seed):
 
 
 def test_sync_find_matches_oracle(ctx):
-    """Partitions without a block header get the oracle's sync start in
-    fixed-Huffman data (or none)."""
+    """Partitions get the oracle's sync start in fixed-Huffman data, searched
+    first, or else its first block-start candidate."""
     for ctype, seed in ((W.MARKOV, 41), (W.RUNS, 42), (W.RAMPS, 43)):
         p, c = _level1(ctype, 3 << 20, seed)
         nbits = c.size * 8
@@ -329,12 +338,7 @@ def test_sync_find_matches_oracle(ctx):
         got = ctx.debug_find(c, ranges)
         n_sync = 0
         for (f, t), g in zip(ranges, got):
-            first, seek = O.find_blocks(c, f, t, cap=1 << 18)
-            if first.size:
-                exp = (int(first[0]), int(seek[0]))
-            else:
-                b = O.fixed_sync_find(c, f, t)
-                exp = ("sync", b) if b is not None else None
+            exp = _expected_start(c, f, t)
             n_sync += exp is not None and exp[0] == "sync"
             assert g == exp, (ctype, f, t, g, exp)
         if ctype != W.RAMPS:
