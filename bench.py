@@ -408,7 +408,7 @@ def bench_serving(args, rank: int, world: int, local: int):
         if mode == "served":
             srv = G.Server(device=local, lanes=args.lanes)
         else:
-            srv = G.Server(device=local, lanes=1, max_batch_requests=1)
+            srv = G.Server(device=local, lanes=1, max_batch_requests=1, small_lanes=-1)
         # warm the lanes' buffers with one pass over the pool
         for tk in [srv.submit(c, out=free[i][0]) for i, c in enumerate(comps)]:
             srv.result(tk, copy=False)
@@ -418,11 +418,17 @@ def bench_serving(args, rank: int, world: int, local: int):
         srv.close()
         tot = np.array([x[0] for x in lat])
         qw = np.array([x[1] for x in lat])
+        # small: outputs under 1 MiB (the 4-256 KiB class of the pool)
+        small = np.array([sizes[i] < (1 << 20) for _, i in arrivals[:len(lat)]])
         res[mode] = {"value": round(offered / wall / 1e9, 4), "unit": "GB/s",
                      "p50_ms": round(float(np.percentile(tot, 50)), 3),
                      "p99_ms": round(float(np.percentile(tot, 99)), 3),
                      "p50_queue_ms": round(float(np.percentile(qw, 50)), 3),
                      "p99_queue_ms": round(float(np.percentile(qw, 99)), 3),
+                     "small_p50_ms": round(float(np.percentile(tot[small], 50)), 3),
+                     "small_p99_ms": round(float(np.percentile(tot[small], 99)), 3),
+                     "large_p50_ms": round(float(np.percentile(tot[~small], 50)), 3),
+                     "large_p99_ms": round(float(np.percentile(tot[~small], 99)), 3),
                      "requests": len(lat), "batches": int(st.batches), "byte_exact_sample": ok,
                      "checked": n_checked, "wall_s": round(wall, 2), "clocks": clk.summary()}
     line = {"metric": METRIC, "value": res["served"]["value"], "unit": "GB/s", "n_gpus": world,
@@ -563,7 +569,7 @@ def main():
     ap.add_argument("--rate", type=float, default=0.0, help="serving: arrivals/s (0 = 60%% of capacity)")
     ap.add_argument("--duration", type=float, default=60.0, help="serving: seconds of arrivals")
     ap.add_argument("--pool", type=int, default=64, help="serving: distinct requests")
-    ap.add_argument("--lanes", type=int, default=3, help="serving: concurrent batches")
+    ap.add_argument("--lanes", type=int, default=4, help="serving: concurrent batches")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))

@@ -80,7 +80,7 @@ class Stats(ctypes.Structure):
 
 class ServerConfig(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("lanes", ctypes.c_int), ("autotune", ctypes.c_int),
-                ("pad", ctypes.c_int), ("budget_bytes", ctypes.c_size_t),
+                ("small_lanes", ctypes.c_int), ("budget_bytes", ctypes.c_size_t),
                 ("max_batch_bytes", ctypes.c_size_t), ("max_batch_requests", ctypes.c_size_t),
                 ("large_bytes", ctypes.c_size_t)]
 
@@ -442,11 +442,11 @@ class Server:
     their own CUDA streams) that overlap on the GPU, admitted against a
     device-memory budget; small requests share batches."""
 
-    def __init__(self, device: int = 0, lanes: int = 3, budget_bytes: int = 0,
+    def __init__(self, device: int = 0, lanes: int = 4, budget_bytes: int = 0,
                  max_batch_bytes: int = 0, max_batch_requests: int = 0, large_bytes: int = 0,
-                 autotune: bool = False):
+                 autotune: bool = False, small_lanes: int = 0):
         self._lib = lib()
-        cfg = ServerConfig(device, lanes, int(autotune), 0, budget_bytes, max_batch_bytes,
+        cfg = ServerConfig(device, lanes, int(autotune), small_lanes, budget_bytes, max_batch_bytes,
                            max_batch_requests, large_bytes)
         h = ctypes.c_void_p()
         rc = self._lib.gzgpu_server_create(ctypes.byref(h), ctypes.byref(cfg))

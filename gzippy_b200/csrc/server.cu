@@ -13,7 +13,9 @@
 //     large one (compressed size >= large_bytes) runs alone, otherwise the
 //     lane merges the small requests behind it (up to max_batch_bytes of
 //     input) into one gzgpu_decompress_batch job, i.e. one persistent decode
-//     launch.  Lanes run concurrently, so requests that arrive while others
+//     launch.  `small_lanes` lanes take only small requests (passing large
+//     ones by), so small requests do not wait while large ones hold every
+//     lane.  Lanes run concurrently, so requests that arrive while others
 //     are on the GPU start as soon as a lane and budget free up, and their
 //     kernels overlap with the batches already running.
 #include <chrono>
@@ -68,6 +70,34 @@ struct gzgpu_server {
     const Request* r = queue.front();
     return budget_used + r->charge <= cfg.budget_bytes;
   }
+  // a small request (in FIFO order among the small ones) that fits the budget
+  bool admissible_small() const {
+    for (const Request* r : queue)
+      if (r->in_len < cfg.large_bytes) return budget_used + r->charge <= cfg.budget_bytes;
+    return false;
+  }
+  // pop the small requests at the front of the small ones (caller holds mu);
+  // the lanes reserved for small requests take these, passing large ones by
+  void take_small_batch(std::vector<Request*>& b) {
+    b.clear();
+    size_t in_total = 0;
+    const auto now = Clock::now();
+    for (auto it = queue.begin(); it != queue.end();) {
+      Request* r = *it;
+      if (r->in_len >= cfg.large_bytes) {
+        ++it;
+        continue;
+      }
+      if (!b.empty() && in_total + r->in_len > cfg.max_batch_bytes) break;
+      if (budget_used + r->charge > cfg.budget_bytes) break;
+      it = queue.erase(it);
+      budget_used += r->charge;
+      r->t_admit = now;
+      b.push_back(r);
+      in_total += r->in_len;
+      if (b.size() >= cfg.max_batch_requests) break;
+    }
+  }
 
   // pop the next batch (caller holds mu)
   void take_batch(std::vector<Request*>& b) {
@@ -90,6 +120,7 @@ struct gzgpu_server {
 
   void lane_main(int lane) {
     gzgpu_ctx* ctx = ctxs[lane];
+    const bool small_only = lane < cfg.small_lanes;
     std::vector<Request*> batch;
     std::vector<gzgpu_span> spans;
     std::vector<gzgpu_out> outs;
@@ -97,9 +128,10 @@ struct gzgpu_server {
     for (;;) {
       {
         std::unique_lock<std::mutex> lk(mu);
-        cv_work.wait(lk, [&] { return stop || admissible(); });
+        cv_work.wait(lk, [&] { return stop || (small_only ? admissible_small() : admissible()); });
         if (stop) return;
-        take_batch(batch);
+        if (small_only) take_small_batch(batch);
+        else take_batch(batch);
         st.batches++;
         st.in_flight += batch.size();
       }
@@ -129,7 +161,7 @@ struct gzgpu_server {
         st.in_flight -= batch.size();
       }
       cv_done.notify_all();
-      cv_work.notify_all();
+      cv_work.notify_all();  // budget freed: any lane may admit now
     }
   }
 };
@@ -143,7 +175,9 @@ int gzgpu_server_create(gzgpu_server** out, const gzgpu_server_config* cfg) {
   if (!s) return GZGPU_DEVICE_ERROR;
   if (cfg) s->cfg = *cfg;
   if (!s->cfg.budget_bytes) s->cfg.budget_bytes = 120ull << 30;
-  if (s->cfg.lanes <= 0) s->cfg.lanes = 3;
+  if (s->cfg.lanes <= 0) s->cfg.lanes = 4;
+  if (s->cfg.small_lanes == 0) s->cfg.small_lanes = s->cfg.lanes >= 2 ? 1 : 0;
+  if (s->cfg.small_lanes < 0 || s->cfg.small_lanes >= s->cfg.lanes) s->cfg.small_lanes = 0;
   if (!s->cfg.max_batch_bytes) s->cfg.max_batch_bytes = 256ull << 20;
   if (!s->cfg.max_batch_requests) s->cfg.max_batch_requests = 4096;
   if (!s->cfg.large_bytes) s->cfg.large_bytes = 32ull << 20;
@@ -201,7 +235,9 @@ int gzgpu_submit(gzgpu_server* s, const uint8_t* in, size_t in_len, uint8_t* out
     s->st.submitted++;
   }
   *ticket = r->id;
-  s->cv_work.notify_one();
+  // every lane: a lane reserved for small requests does not take a large one,
+  // so waking only one could leave the request queued with a general lane idle
+  s->cv_work.notify_all();
   return GZGPU_OK;
 }
 

@@ -174,15 +174,17 @@ int gzgpu_decompress_device_noalloc(const void *d_in, size_t in_len, void *d_out
  * and decoder pages) fits the device-memory budget next to the requests in
  * flight; the queue is FIFO.  A request of at least large_bytes compressed
  * runs alone; smaller ones are merged, up to max_batch_bytes of input, into
- * one batch (one gzgpu_decompress_batch job).  Inputs and outputs are the
+ * one batch (one gzgpu_decompress_batch job).  small_lanes of the lanes take
+ * only small requests, so these never wait behind large ones.  Inputs and outputs are the
  * caller's and must stay valid until the request has been polled done. */
 typedef struct gzgpu_server gzgpu_server;
 
 typedef struct {
   int device;
-  int lanes;                 /* concurrent batches; 0 = 3 */
+  int lanes;                 /* concurrent batches; 0 = 4 */
   int autotune;              /* the lanes' contexts use the autotuner */
-  int pad;
+  int small_lanes;           /* lanes that take only small requests; 0 = 1 (with 2+ lanes),
+                                -1 = none */
   size_t budget_bytes;       /* device-memory budget of admitted requests; 0 = 120 GB */
   size_t max_batch_bytes;    /* compressed bytes merged into one batch; 0 = 256 MiB */
   size_t max_batch_requests; /* requests merged into one batch; 0 = 4096 */

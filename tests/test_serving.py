@@ -107,3 +107,34 @@ def test_poll_pending_then_done():
     with pytest.raises(Exception):
         srv.result(tk)                     # a collected ticket is released
     srv.close()
+
+
+def test_small_requests_pass_large_ones():
+    """With one lane reserved for small requests, small requests submitted
+    behind a queue of large ones finish before the last large one (which
+    waits for the large ones ahead of it on the general lane)."""
+    import gzippy_b200 as G
+    large = [W.gzip_member(W.content(W.MARKOV, 500 + k, 48 << 20), 1).tobytes() for k in range(3)]
+    small = [W.gzip_member(W.content(k % 4, 600 + k, 64 << 10), 6).tobytes() for k in range(16)]
+    srv = G.Server(lanes=2, small_lanes=1, large_bytes=4 << 20)
+    assert all(len(c) >= 4 << 20 for c in large)
+    wait = 120_000                         # ms; a request left queued fails, not hangs
+    for c in small[:2] + large[:1]:        # first use of both lanes' buffers
+        rc, _, _ = srv.poll(srv.submit(c), wait)
+        assert rc == G.OK
+    tl = [srv.submit(c) for c in large]
+    ts = [srv.submit(c) for c in small]
+    small_ms = []
+    for c, tk in zip(small, ts):
+        rc, data, tm = srv.poll(tk, wait)
+        assert rc == G.OK and data == zlib.decompress(c, 31)
+        small_ms.append(tm.total_ms)
+    large_ms = []
+    for c, tk in zip(large, tl):
+        rc, data, tm = srv.poll(tk, wait)
+        assert rc == G.OK and data == zlib.decompress(c, 31)
+        large_ms.append(tm.total_ms)
+    assert max(small_ms) < large_ms[-1], (small_ms, large_ms)
+    s = srv.stats()
+    assert s.in_flight == 0 and s.queued == 0 and s.budget_used == 0
+    srv.close()
