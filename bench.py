@@ -305,8 +305,10 @@ def bench_batch(args, rank: int, world: int, local: int):
 
 def run_trace(srv, comps, sizes, crcs, arrivals, free, verify_every: int = 8):
     """Replay arrivals (t, pool index) against a Server; returns per-request
-    (total_ms, queue_ms), wall seconds from the first arrival to the last
-    completion, and whether the sampled outputs matched."""
+    (total_ms, queue_ms) in arrival order, wall seconds from the first arrival
+    to the last completion, and whether the sampled outputs matched.  Results
+    are collected as they complete (not in arrival order), so each output
+    buffer returns to the pool as soon as its request is done."""
     import threading
     import zlib
     import gzippy_b200 as G
@@ -326,20 +328,31 @@ def run_trace(srv, comps, sizes, crcs, arrivals, free, verify_every: int = 8):
 
     th = threading.Thread(target=submitter)
     th.start()
-    lat, ok, n_checked = [], True, 0
-    for k in range(len(arrivals)):
-        while tickets[k] is None:
-            time.sleep(0.0005)
-        tk, i, out = tickets[k]
-        rc, data, tm = srv.poll(tk, -1, copy=False)
-        if rc != G.OK or len(data) != int(sizes[i]):
-            ok = False
-        elif k % verify_every == 0:
-            n_checked += 1
-            ok &= zlib.crc32(data) == crcs[i]
-        lat.append((tm.total_ms, tm.queue_ms))
-        with lock:
-            free.setdefault(i, []).append(out)
+    lat, ok, n_checked = [None] * len(arrivals), True, 0
+    pending, seen, n_done = {}, 0, 0
+    while n_done < len(arrivals):
+        while seen < len(arrivals) and tickets[seen] is not None:
+            pending[seen] = tickets[seen]
+            seen += 1
+        progressed = False
+        for k in list(pending):
+            tk, i, out = pending[k]
+            rc, data, tm = srv.poll(tk, 0, copy=False)
+            if rc == G.PENDING:
+                continue
+            if rc != G.OK or len(data) != int(sizes[i]):
+                ok = False
+            elif k % verify_every == 0:
+                n_checked += 1
+                ok &= zlib.crc32(data) == crcs[i]
+            lat[k] = (tm.total_ms, tm.queue_ms)
+            with lock:
+                free.setdefault(i, []).append(out)
+            del pending[k]
+            n_done += 1
+            progressed = True
+        if not progressed:
+            time.sleep(0.0002)
     th.join()
     wall = time.perf_counter() - t0
     return lat, wall, ok, n_checked

@@ -52,7 +52,7 @@ class Config(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("chunk_bytes", ctypes.c_size_t),
                 ("lut_bits", ctypes.c_int), ("autotune", ctypes.c_int),
                 ("ring_history", ctypes.c_int), ("ctas_per_sm", ctypes.c_int),
-                ("fine_split", ctypes.c_int)]
+                ("fine_split", ctypes.c_int), ("high_priority", ctypes.c_int)]
 
 
 class Span(ctypes.Structure):
@@ -168,10 +168,10 @@ class Context:
 
     def __init__(self, device: int = 0, chunk_bytes: int = 0, lut_bits: int = 0,
                  autotune: bool = False, ring_history: bool = False, ctas_per_sm: int = 0,
-                 fine_split: bool = False):
+                 fine_split: bool = False, high_priority: bool = False):
         self._lib = lib()
         cfg = Config(device, chunk_bytes, lut_bits, int(autotune), int(ring_history), ctas_per_sm,
-                     int(fine_split))
+                     int(fine_split), int(high_priority))
         h = ctypes.c_void_p()
         rc = self._lib.gzgpu_create(ctypes.byref(h), ctypes.byref(cfg))
         if rc != OK:

@@ -30,6 +30,7 @@
 #include "inflate.cuh"
 #include "members.cuh"
 #include "resolve.cuh"
+#include "stage.h"
 
 using namespace gzgpu;
 
@@ -166,9 +167,11 @@ struct gzgpu_ctx {
   bool ring = false;  // history layout of the inflate kernel (false = pages)
   int ctas_per_sm = 3;  // page kernel CTAs per SM (3 or 4)
   bool fine_split = false;  // output-estimate pieces + dynamic-block sync starts
+  bool high_priority = false;  // stream at the device's greatest priority
   bool job_sync = true;     // the running job has sync starts (decoder variant)
   int decode_blocks = 0;
   cudaEvent_t ev[12];
+  cudaEvent_t stage_ev[2];  // last DMA of each pinned staging slot
   gzgpu_stats stats{};
   bool crc_ready = false;
 
@@ -1101,17 +1104,22 @@ int gzgpu_create(gzgpu_ctx** out, const gzgpu_config* cfg) {
     c->ring = cfg->ring_history != 0;
     if (cfg->ctas_per_sm == 3 || cfg->ctas_per_sm == 4) c->ctas_per_sm = cfg->ctas_per_sm;
     c->fine_split = cfg->fine_split != 0;
+    c->high_priority = cfg->high_priority != 0;
   }
   if (cudaSetDevice(c->dev) != cudaSuccess) {
     delete c;
     return GZGPU_DEVICE_ERROR;
   }
   cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, c->dev);
-  if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess) {
+  int prio_least = 0, prio_greatest = 0;
+  cudaDeviceGetStreamPriorityRange(&prio_least, &prio_greatest);
+  if (cudaStreamCreateWithPriority(&c->st, cudaStreamNonBlocking,
+                                   c->high_priority ? prio_greatest : prio_least) != cudaSuccess) {
     delete c;
     return GZGPU_DEVICE_ERROR;
   }
   for (auto& e : c->ev) cudaEventCreate(&e);
+  for (auto& e : c->stage_ev) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
   for (DevBuf* b : c->all_bufs()) b->st = c->st;
   {
     // keep memory freed by buffer growth in the device's pool for reuse
@@ -1134,6 +1142,7 @@ void gzgpu_destroy(gzgpu_ctx* c) {
   cudaStreamSynchronize(c->st);
   c->h_stage.release();
   for (auto& e : c->ev) cudaEventDestroy(e);
+  for (auto& e : c->stage_ev) cudaEventDestroy(e);
   cudaStreamDestroy(c->st);
   delete c;
 }
@@ -1252,22 +1261,32 @@ int gzgpu_decompress_to_writer(gzgpu_ctx* c, const uint8_t* in, size_t in_len,
   if (rc != kOk) return rc;
   finish_stats(c);
   if (R[0].status != kOk) return R[0].status;
-  // deliver in order through a pinned bounce buffer, two halves in flight
-  const size_t piece = 32 << 20;
+  // deliver in order through the pinned staging ring: the next piece
+  // downloads while the writer consumes this one
+  const size_t piece = kStageSlot;
   if (!c->h_stage.ensure(2 * piece)) return GZGPU_DEVICE_ERROR;
   uint8_t* hb = reinterpret_cast<uint8_t*>(c->h_stage.p);
-  uint64_t done = 0, total = R[0].out_len;
-  int half = 0;
-  while (done < total) {
-    size_t k = (size_t)std::min<uint64_t>(piece, total - done);
-    if ((rc = c->check(cudaMemcpyAsync(hb + half * piece, c->cur_out + R[0].out_off + done, k,
-                                       cudaMemcpyDeviceToHost, c->st))))
-      return rc;
-    if ((rc = c->check(cudaStreamSynchronize(c->st)))) return rc;
-    if (write(user, hb + half * piece, k) != 0) return GZGPU_INVALID_ARGUMENT;
-    done += k;
-    half ^= 1;
-    if (written) *written = done;
+  const uint64_t total = R[0].out_len;
+  // piece i goes to half i % 2; piece i + 1 downloads while piece i is written
+  auto issue = [&](uint64_t at) -> int {
+    const int half = (int)((at / piece) & 1);
+    const size_t k = (size_t)std::min<uint64_t>(piece, total - at);
+    int e = c->check(cudaMemcpyAsync(hb + half * piece, c->cur_out + R[0].out_off + at, k,
+                                     cudaMemcpyDeviceToHost, c->st));
+    return e ? e : c->check(cudaEventRecord(c->stage_ev[half], c->st));
+  };
+  for (uint64_t at = 0; at < total && at < 2 * piece; at += piece)
+    if ((rc = issue(at))) return rc;
+  for (uint64_t at = 0; at < total; at += piece) {
+    const int half = (int)((at / piece) & 1);
+    const size_t k = (size_t)std::min<uint64_t>(piece, total - at);
+    if ((rc = c->check(cudaEventSynchronize(c->stage_ev[half])))) return rc;
+    if (write(user, hb + half * piece, k) != 0) {
+      cudaStreamSynchronize(c->st);  // no download into the ring outlives the call
+      return GZGPU_INVALID_ARGUMENT;
+    }
+    if (written) *written = at + k;
+    if (at + 2 * piece < total && (rc = issue(at + 2 * piece))) return rc;
   }
   return GZGPU_OK;
 }
@@ -1312,8 +1331,9 @@ namespace {
 
 // Host copies of the batch path: a stream of at least kDirectBytes in
 // page-locked memory moves by DMA straight from / to the caller's buffer;
-// the others go through the context's pinned staging buffer, copied by up
-// to kCopyThreads host threads.
+// the others go through the context's pinned staging ring (stage.h: two
+// kStageSlot slots, allocated once), gathered and scattered by up to
+// kCopyThreads host threads while the other slot's DMA runs.
 constexpr size_t kDirectBytes = 1u << 20;
 constexpr int kCopyThreads = 8;
 
@@ -1360,6 +1380,43 @@ void parallel_copy(const std::vector<CopyJob>& jobs) {
   for (std::thread& x : th) x.join();
 }
 
+// the staging ring's device side: copies and slot events on the context stream
+struct CudaStageOps {
+  gzgpu_ctx* c;
+  uint8_t* dev;  // device base of the staged byte offsets
+  int to_dev(uint64_t d, const uint8_t* src, uint64_t len) {
+    return c->check(cudaMemcpyAsync(dev + d, src, len, cudaMemcpyHostToDevice, c->st));
+  }
+  int to_host(uint8_t* dst, uint64_t d, uint64_t len) {
+    return c->check(cudaMemcpyAsync(dst, dev + d, len, cudaMemcpyDeviceToHost, c->st));
+  }
+  int record(int sl) { return c->check(cudaEventRecord(c->stage_ev[sl], c->st)); }
+  int wait(int sl) { return c->check(cudaEventSynchronize(c->stage_ev[sl])); }
+  void gather(const std::vector<StageHost>& h, uint8_t* slot) {
+    std::vector<CopyJob> jobs;
+    for (const StageHost& x : h) jobs.push_back(CopyJob{slot + x.slot_off, x.host, x.len});
+    parallel_copy(jobs);
+  }
+  void scatter(const std::vector<StageHost>& h, const uint8_t* slot) {
+    std::vector<CopyJob> jobs;
+    for (const StageHost& x : h) jobs.push_back(CopyJob{x.host, slot + x.slot_off, x.len});
+    parallel_copy(jobs);
+  }
+};
+
+// run the ring over `fills` (upload: host -> dev, else dev -> host); on
+// failure wait for the stream, so that no copy into or out of the ring
+// outlives the call
+int staged(gzgpu_ctx* c, const std::vector<StageFill>& fills, uint8_t* dev, bool upload) {
+  if (!c->h_stage.ensure(2 * kStageSlot)) return GZGPU_DEVICE_ERROR;
+  uint8_t* hb = reinterpret_cast<uint8_t*>(c->h_stage.p);
+  uint8_t* const slots[2] = {hb, hb + kStageSlot};
+  CudaStageOps ops{c, dev};
+  const int rc = upload ? stage_upload(fills, slots, ops) : stage_download(fills, slots, ops);
+  if (rc) cudaStreamSynchronize(c->st);
+  return rc;
+}
+
 }  // namespace
 
 int gzgpu_decompress_batch(gzgpu_ctx* c, const gzgpu_span* ins, size_t n, gzgpu_out* outs,
@@ -1372,54 +1429,39 @@ int gzgpu_decompress_batch(gzgpu_ctx* c, const gzgpu_span* ins, size_t n, gzgpu_
   for (size_t i = 0; i < n; i++) total += (ins[i].len + 15) & ~15ull;
   int rc;
   if ((rc = c->check(c->in.ensure(total + kInputPad)))) return rc;
-  // pack the streams (16-byte aligned): staged ones into the pinned buffer
+  // pack the streams (16-byte aligned): direct ones by DMA from the caller's
+  // page-locked buffers, the others through the staging ring
   std::vector<StreamSpec> S(n);
   std::vector<char> direct(n, 0);
-  std::vector<CopyJob> jobs;
-  uint64_t at = 0, staged = 0;
+  uint64_t at = 0;
   for (size_t i = 0; i < n; i++) {
     S[i] = StreamSpec{at, ins[i].len};
     direct[i] = ins[i].len >= kDirectBytes && host_pinned(ins[i].data);
-    if (!direct[i]) staged += ins[i].len;
     at += (ins[i].len + 15) & ~15ull;
   }
-  // runs of consecutive staged streams: each is laid out in the staging
-  // buffer as on the device and uploaded by one copy
-  struct Run {
-    size_t i, j;
-    uint64_t stage_off;
-  };
-  std::vector<Run> runs;
-  uint64_t stage_total = 0;
+  // runs of consecutive staged streams: device ranges (alignment gaps
+  // included) that the ring uploads piece by piece
+  std::vector<StageSeg> segs;
+  std::vector<StageRun> runs;
   for (size_t i = 0; i < n;) {
     if (direct[i]) {
       i++;
       continue;
     }
+    const size_t s0 = segs.size();
     size_t j = i;
-    while (j < n && !direct[j]) j++;
-    runs.push_back(Run{i, j, stage_total});
-    stage_total += S[j - 1].off + S[j - 1].len - S[i].off;
+    for (; j < n && !direct[j]; j++)
+      segs.push_back(StageSeg{const_cast<uint8_t*>(ins[j].data), S[j].off, ins[j].len});
+    runs.push_back(StageRun{S[i].off, S[j - 1].off + S[j - 1].len, s0, segs.size()});
     i = j;
   }
-  if (!c->h_stage.ensure(stage_total ? stage_total : 1)) return GZGPU_DEVICE_ERROR;
-  uint8_t* hb = reinterpret_cast<uint8_t*>(c->h_stage.p);
-  for (const Run& r : runs)
-    for (size_t k = r.i; k < r.j; k++)
-      if (ins[k].len)
-        jobs.push_back(CopyJob{hb + r.stage_off + (S[k].off - S[r.i].off), ins[k].data, ins[k].len});
-  parallel_copy(jobs);
   cudaEventRecord(c->ev[0], c->st);
   uint8_t* din = c->in.as<uint8_t>();
   for (size_t i = 0; i < n; i++)
-    if (direct[i])
-      cudaMemcpyAsync(din + S[i].off, ins[i].data, ins[i].len, cudaMemcpyHostToDevice, c->st);
-  for (const Run& r : runs) {
-    const uint64_t r0 = S[r.i].off, r1 = S[r.j - 1].off + S[r.j - 1].len;
-    if (r1 > r0 && (rc = c->check(cudaMemcpyAsync(din + r0, hb + r.stage_off, r1 - r0,
-                                                  cudaMemcpyHostToDevice, c->st))))
+    if (direct[i] && (rc = c->check(cudaMemcpyAsync(din + S[i].off, ins[i].data, ins[i].len,
+                                                    cudaMemcpyHostToDevice, c->st))))
       return rc;
-  }
+  if (!runs.empty() && (rc = staged(c, stage_plan(segs, runs), din, true))) return rc;
   cudaMemsetAsync(din + at, 0, kInputPad, c->st);
   c->cur_in = din;
   c->user_out = nullptr;
@@ -1430,7 +1472,6 @@ int gzgpu_decompress_batch(gzgpu_ctx* c, const gzgpu_span* ins, size_t n, gzgpu_
   int all = GZGPU_OK;
   cudaEvent_t t0 = c->ev[8], t1 = c->ev[9];
   cudaEventRecord(t0, c->st);
-  jobs.clear();
   std::vector<char> deliver(n, 0);
   for (size_t i = 0; i < n; i++) {
     statuses[i] = R[i].status;
@@ -1444,41 +1485,35 @@ int gzgpu_decompress_batch(gzgpu_ctx* c, const gzgpu_span* ins, size_t n, gzgpu_
     if (statuses[i] != GZGPU_OK && statuses[i] != GZGPU_NOT_GZIP && all == GZGPU_OK) all = statuses[i];
   }
   // outputs: large ones into page-locked caller memory by DMA; the rest in
-  // runs contiguous on the device, one download each into the staging buffer
+  // runs contiguous on the device, downloaded through the staging ring
   std::vector<char> odirect(n, 0);
-  runs.clear();
-  stage_total = 0;
   for (size_t i = 0; i < n; i++)
     odirect[i] = deliver[i] && R[i].out_len >= kDirectBytes && host_pinned(outs[i].data);
+  segs.clear();
+  runs.clear();
   for (size_t i = 0; i < n;) {
     if (!deliver[i] || odirect[i]) {
       i++;
       continue;
     }
-    size_t j = i + 1;
-    while (j < n && deliver[j] && !odirect[j] && R[j].out_off == R[j - 1].out_off + R[j - 1].out_len)
+    const size_t s0 = segs.size();
+    size_t j = i;
+    do {
+      segs.push_back(StageSeg{outs[j].data, R[j].out_off, R[j].out_len});
       j++;
-    runs.push_back(Run{i, j, stage_total});
-    stage_total += R[j - 1].out_off + R[j - 1].out_len - R[i].out_off;
+    } while (j < n && deliver[j] && !odirect[j] && R[j].out_off == R[j - 1].out_off + R[j - 1].out_len);
+    runs.push_back(StageRun{R[i].out_off, R[j - 1].out_off + R[j - 1].out_len, s0, segs.size()});
     i = j;
   }
-  if (!c->h_stage.ensure(stage_total ? stage_total : 1)) return GZGPU_DEVICE_ERROR;
-  hb = reinterpret_cast<uint8_t*>(c->h_stage.p);
   for (size_t i = 0; i < n; i++)
-    if (odirect[i])
-      cudaMemcpyAsync(outs[i].data, c->cur_out + R[i].out_off, R[i].out_len, cudaMemcpyDeviceToHost,
-                      c->st);
-  for (const Run& r : runs) {
-    const uint64_t r0 = R[r.i].out_off, r1 = R[r.j - 1].out_off + R[r.j - 1].out_len;
-    if ((rc = c->check(cudaMemcpyAsync(hb + r.stage_off, c->cur_out + r0, r1 - r0,
-                                       cudaMemcpyDeviceToHost, c->st))))
+    if (odirect[i] && (rc = c->check(cudaMemcpyAsync(outs[i].data, c->cur_out + R[i].out_off,
+                                                     R[i].out_len, cudaMemcpyDeviceToHost, c->st)))) {
+      cudaStreamSynchronize(c->st);
       return rc;
-    for (size_t k = r.i; k < r.j; k++)
-      jobs.push_back(CopyJob{outs[k].data, hb + r.stage_off + (R[k].out_off - r0), R[k].out_len});
-  }
+    }
+  if (!runs.empty() && (rc = staged(c, stage_plan(segs, runs), c->cur_out, false))) return rc;
   cudaEventRecord(t1, c->st);
   if ((rc = c->check(cudaStreamSynchronize(c->st)))) return rc;
-  parallel_copy(jobs);
   float t = 0;
   cudaEventElapsedTime(&t, t0, t1);
   c->stats.ms_d2h = t;

@@ -15,7 +15,8 @@
 //     input) into one gzgpu_decompress_batch job, i.e. one persistent decode
 //     launch.  `small_lanes` lanes take only small requests (passing large
 //     ones by), so small requests do not wait while large ones hold every
-//     lane.  Lanes run concurrently, so requests that arrive while others
+//     lane; their streams have the device's greatest priority, so their
+//     thread blocks are scheduled before the large jobs' pending ones.  Lanes run concurrently, so requests that arrive while others
 //     are on the GPU start as soon as a lane and budget free up, and their
 //     kernels overlap with the batches already running.
 #include <chrono>
@@ -185,6 +186,8 @@ int gzgpu_server_create(gzgpu_server** out, const gzgpu_server_config* cfg) {
     gzgpu_config c{};
     c.device = s->cfg.device;
     c.autotune = s->cfg.autotune;
+    // small requests' kernels go ahead of large ones' pending blocks
+    c.high_priority = i < s->cfg.small_lanes;
     gzgpu_ctx* ctx = nullptr;
     int rc = gzgpu_create(&ctx, &c);
     if (rc != GZGPU_OK) {

@@ -59,7 +59,7 @@ typedef struct {
                          is decoded once per candidate and the fastest is kept for
                          later jobs of that kind; overrides the three fields */
   int ring_history;   /* 1 = decode history in a shared-memory ring (3 warps/SM) instead
-                         of the output pages in HBM (32 warps/SM, the default) */
+                         of the output pages in HBM (24 or 32 warps/SM, the default) */
   int ctas_per_sm;    /* page-history decoder: 3 (24 warps/SM, 80 registers; default) or
                          4 (32 warps/SM, 64 registers); 0 = default */
   int fine_split;     /* 1 = cut partitions whose first blocks promise a high output
@@ -67,6 +67,9 @@ typedef struct {
                          sync start inside their dynamic block; 0 = off (default:
                          measured no faster on the mixed, multi-member and batch
                          workloads) */
+  int high_priority;  /* 1 = the context's stream has the device's greatest priority:
+                         its pending thread blocks are scheduled before those of other
+                         contexts' streams (running blocks are not preempted) */
 } gzgpu_config;
 
 typedef struct {
