@@ -121,6 +121,7 @@ def lib():
             L.gzgpu_strerror.restype = ctypes.c_char_p
             L.gzgpu_decompress.argtypes = [vp, vp, sz, vp, sz, ctypes.POINTER(sz)]
             L.gzgpu_decompress_device.argtypes = [vp, vp, sz, vp, sz, ctypes.POINTER(sz)]
+            L.gzgpu_inflate_raw.argtypes = [vp, vp, sz, vp, sz, ctypes.POINTER(sz)]
             L.gzgpu_decompress_to_writer.argtypes = [vp, vp, sz, WRITE_FN, vp,
                                                      ctypes.POINTER(ctypes.c_uint64)]
             u64p = ctypes.POINTER(ctypes.c_uint64)
@@ -219,6 +220,27 @@ class Context:
                                             ctypes.byref(n))
             if rc == NOT_GZIP:
                 return b""
+            if rc == OUT_TOO_SMALL:
+                cap = n.value
+                continue
+            if rc != OK:
+                _raise(rc)
+            return out[:n.value].tobytes()
+        _raise(OUT_TOO_SMALL)
+
+    def inflate_raw(self, data) -> bytes:
+        """One raw DEFLATE stream (gzippy::decompress_raw, src/lib.rs:250):
+        decoded up to its final block, trailing bytes ignored; raises on
+        invalid or cut-off data.  The first output guess is 4x the input, as
+        in decompress_raw_bytes (src/decompress/mod.rs:920); a short guess is
+        retried once at the exact size."""
+        a = _as_u8(data)
+        cap = max(4096, a.size * 4)
+        for _ in range(2):
+            out = np.empty(cap, dtype=np.uint8)
+            n = ctypes.c_size_t(0)
+            rc = self._lib.gzgpu_inflate_raw(self._h, a.ctypes.data, a.size, out.ctypes.data, cap,
+                                             ctypes.byref(n))
             if rc == OUT_TOO_SMALL:
                 cap = n.value
                 continue
@@ -404,6 +426,14 @@ def decompress(data) -> bytes:
 def decompress_with_threads(data, threads: int) -> bytes:
     """gzippy::decompress_with_threads (src/lib.rs:189)."""
     return _ctx().decompress(data)
+
+
+def decompress_raw(data) -> bytes:
+    """gzippy::decompress_raw (src/lib.rs:250): one raw DEFLATE stream."""
+    return _ctx().inflate_raw(data)
+
+
+deflate_decode = decompress_raw  # the reference's alias (src/lib.rs:258)
 
 
 def decompress_to_writer(data, writer) -> int:

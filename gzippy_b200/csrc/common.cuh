@@ -20,6 +20,7 @@ constexpr uint32_t kPageEntries = 65536;     // u16 entries per output page
 constexpr uint32_t kFlush = 8192;            // ring -> page flush unit (entries)
 constexpr uint32_t kInputPad = 1024;         // zero bytes after the input buffer
 constexpr uint64_t kNoStop = ~0ull;
+constexpr uint64_t kNoTrailer = ~0ull;  // a member without CRC32/ISIZE (raw DEFLATE)
 constexpr uint32_t kNoPage = 0xFFFFFFFFu;
 
 // status codes (same numbering as include/gzgpu.h)

@@ -168,6 +168,7 @@ struct gzgpu_ctx {
   int ctas_per_sm = 3;  // page kernel CTAs per SM (3 or 4)
   bool fine_split = false;  // output-estimate pieces + dynamic-block sync starts
   bool high_priority = false;  // stream at the device's greatest priority
+  bool job_raw = false;        // the job's streams are raw DEFLATE (no gzip framing)
   bool job_sync = true;     // the running job has sync starts (decoder variant)
   int decode_blocks = 0;
   cudaEvent_t ev[12];
@@ -357,20 +358,26 @@ int gzgpu_ctx::run(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R) 
     cudaMemcpyAsync(this->units.p, units.data(), sizeof(ScanUnit) * units.size(),
                     cudaMemcpyHostToDevice, st);
   cudaMemsetAsync(counters.p, 0, 64, st);
-  if ((rc = check(launch_stream_headers(cur_in, s_off.as<uint64_t>(), s_len.as<uint64_t>(),
-                                        ns, info.as<StreamInfo>(), st))))
-    return rc;
-  if ((rc = check(launch_member_scan(cur_in, this->units.as<ScanUnit>(),
-                                     (uint32_t)units.size(), s_off.as<uint64_t>(),
-                                     s_len.as<uint64_t>(), info.as<StreamInfo>(),
-                                     cands.as<MemberCand>(), counters.as<uint32_t>(), cand_cap, sms,
-                                     st))))
-    return rc;
-  stats.kernel_launches += 2;
   std::vector<StreamInfo> hinfo(ns);
   uint32_t n_cand = 0;
-  cudaMemcpyAsync(hinfo.data(), info.p, sizeof(StreamInfo) * ns, cudaMemcpyDeviceToHost, st);
-  cudaMemcpyAsync(&n_cand, counters.p, 4, cudaMemcpyDeviceToHost, st);
+  if (job_raw) {
+    // raw DEFLATE: no header to check and no members to find; each stream
+    // is one member whose data starts at its first bit
+    for (StreamInfo& h : hinfo) h = StreamInfo{kOk, 0, 0, 4};
+  } else {
+    if ((rc = check(launch_stream_headers(cur_in, s_off.as<uint64_t>(), s_len.as<uint64_t>(),
+                                          ns, info.as<StreamInfo>(), st))))
+      return rc;
+    if ((rc = check(launch_member_scan(cur_in, this->units.as<ScanUnit>(),
+                                       (uint32_t)units.size(), s_off.as<uint64_t>(),
+                                       s_len.as<uint64_t>(), info.as<StreamInfo>(),
+                                       cands.as<MemberCand>(), counters.as<uint32_t>(), cand_cap,
+                                       sms, st))))
+      return rc;
+    stats.kernel_launches += 2;
+    cudaMemcpyAsync(hinfo.data(), info.p, sizeof(StreamInfo) * ns, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(&n_cand, counters.p, 4, cudaMemcpyDeviceToHost, st);
+  }
   if ((rc = check(cudaStreamSynchronize(st)))) return rc;
   cudaEventRecord(ev[2], st);
   if (autotune) {
@@ -448,6 +455,7 @@ int gzgpu_ctx::run(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R) 
       ms.push_back(Mem{0, hinfo[s].header_len, len, hinfo[s].last_isize});
     }
     for (auto& m : ms) est_out += m.isize;
+    if (job_raw) est_out += 4 * len;  // no ISIZE: the page pool grows if this is short
     mems[s] = std::move(ms);
   }
   // grid
@@ -772,6 +780,13 @@ int gzgpu_ctx::run(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R) 
         w.done = true;
         break;
       }
+      if (r.final_block && job_raw) {
+        // raw DEFLATE ends with its final block; bytes after it are ignored
+        if ((r.end_bit + 7) / 8 > base + len) w.status = kTruncated;
+        else w.members.push_back(MemberPlan{w.member_order_begin, (uint32_t)w.order.size(), kNoTrailer, 0});
+        w.done = true;
+        break;
+      }
       if (r.final_block) {
         uint64_t trailer = (r.end_bit + 7) / 8;
         if (trailer + 8 > base + len) {
@@ -972,7 +987,7 @@ int gzgpu_ctx::run(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R) 
         }
         so += r.out_len;
       }
-      for (uint64_t b = 0; b < mp.out_len; b += kCrcBlock)
+      for (uint64_t b = 0; mp.trailer != kNoTrailer && b < mp.out_len; b += kCrcBlock)
         cblk.push_back(CrcBlock{moff + b, (uint32_t)std::min(kCrcBlock, mp.out_len - b),
                                 (uint32_t)mtrail.size()});
       mblk.push_back((uint32_t)cblk.size());
@@ -1171,12 +1186,11 @@ void finish_stats(gzgpu_ctx* c) {
 
 }  // namespace
 
-int gzgpu_decompress(gzgpu_ctx* c, const uint8_t* in, size_t in_len, uint8_t* out,
-                     size_t out_cap, size_t* out_len) {
-  if (!c || !out_len || (!in && in_len) || (!out && out_cap)) return GZGPU_INVALID_ARGUMENT;
-  *out_len = 0;
-  if (in_len < 2 || in[0] != 0x1f || in[1] != 0x8b) return GZGPU_NOT_GZIP;
-  std::lock_guard<std::mutex> g(c->mu);
+namespace {
+
+// one host stream through a job (caller holds c->mu): upload, decode, download
+int decompress_host(gzgpu_ctx* c, const uint8_t* in, size_t in_len, uint8_t* out,
+                    size_t out_cap, size_t* out_len) {
   cudaSetDevice(c->dev);
   reset_stats(c);
   int rc;
@@ -1209,6 +1223,29 @@ int gzgpu_decompress(gzgpu_ctx* c, const uint8_t* in, size_t in_len, uint8_t* ou
   cudaEventElapsedTime(&t, c->ev[0], t1);
   c->stats.ms_total = t;
   return GZGPU_OK;
+}
+
+}  // namespace
+
+int gzgpu_decompress(gzgpu_ctx* c, const uint8_t* in, size_t in_len, uint8_t* out,
+                     size_t out_cap, size_t* out_len) {
+  if (!c || !out_len || (!in && in_len) || (!out && out_cap)) return GZGPU_INVALID_ARGUMENT;
+  *out_len = 0;
+  if (in_len < 2 || in[0] != 0x1f || in[1] != 0x8b) return GZGPU_NOT_GZIP;
+  std::lock_guard<std::mutex> g(c->mu);
+  return decompress_host(c, in, in_len, out, out_cap, out_len);
+}
+
+int gzgpu_inflate_raw(gzgpu_ctx* c, const uint8_t* in, size_t in_len, uint8_t* out,
+                      size_t out_cap, size_t* out_len) {
+  if (!c || !out_len || (!in && in_len) || (!out && out_cap)) return GZGPU_INVALID_ARGUMENT;
+  *out_len = 0;
+  if (!in_len) return GZGPU_TRUNCATED;  // no final block
+  std::lock_guard<std::mutex> g(c->mu);
+  c->job_raw = true;
+  const int rc = decompress_host(c, in, in_len, out, out_cap, out_len);
+  c->job_raw = false;
+  return rc;
 }
 
 int gzgpu_decompress_device(gzgpu_ctx* c, const void* d_in, size_t in_len, void* d_out,

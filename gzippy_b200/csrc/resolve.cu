@@ -257,11 +257,13 @@ __global__ void crc_members_kernel(const CrcBlock* __restrict__ blocks,
     uint32_t crc = sc[0];
     mem_crc[m] = crc;
     uint64_t t = mem_trailer[m];
-    uint32_t ecrc = in[t] | (in[t + 1] << 8) | ((uint32_t)in[t + 2] << 16) | ((uint32_t)in[t + 3] << 24);
-    uint32_t eisz = in[t + 4] | (in[t + 5] << 8) | ((uint32_t)in[t + 6] << 16) | ((uint32_t)in[t + 7] << 24);
     int32_t st = kOk;
-    if ((uint32_t)mem_len[m] != eisz) st = kSizeMismatch;
-    else if (crc != ecrc) st = kCrcMismatch;
+    if (t != kNoTrailer) {
+      uint32_t ecrc = in[t] | (in[t + 1] << 8) | ((uint32_t)in[t + 2] << 16) | ((uint32_t)in[t + 3] << 24);
+      uint32_t eisz = in[t + 4] | (in[t + 5] << 8) | ((uint32_t)in[t + 6] << 16) | ((uint32_t)in[t + 7] << 24);
+      if ((uint32_t)mem_len[m] != eisz) st = kSizeMismatch;
+      else if (crc != ecrc) st = kCrcMismatch;
+    }
     mem_status[m] = st;
   }
 }

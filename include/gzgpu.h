@@ -109,6 +109,15 @@ const char *gzgpu_strerror(int code);
 int gzgpu_decompress(gzgpu_ctx *ctx, const uint8_t *in, size_t in_len, uint8_t *out,
                      size_t out_cap, size_t *out_len);
 
+/* gzippy::decompress_raw / deflate_decode (src/lib.rs:250; decompress_raw_bytes,
+ * src/decompress/mod.rs:920): one raw DEFLATE stream (RFC 1951, no gzip
+ * header or trailer), decoded up to its final block; bytes after it are
+ * ignored.  No checksum exists to verify.  Empty or cut-off input:
+ * GZGPU_TRUNCATED; invalid DEFLATE: GZGPU_BAD_DEFLATE.  On
+ * GZGPU_OUT_TOO_SMALL *out_len is the size needed. */
+int gzgpu_inflate_raw(gzgpu_ctx *ctx, const uint8_t *in, size_t in_len, uint8_t *out,
+                      size_t out_cap, size_t *out_len);
+
 /* gzippy::decompress_to_writer / _with_threads (src/lib.rs:204,221):
  * output delivered in order through `write` (return 0 to continue, non-zero
  * to abort with GZGPU_INVALID_ARGUMENT); *written = total bytes delivered. */

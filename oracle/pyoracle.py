@@ -146,6 +146,16 @@ def inflate_chunk(data, start_bit: int, stop_lo: int = 2**64 - 1, window=None,
     return st, res, out[:res.out_len].copy()
 
 
+def inflate_raw(data, cap: int | None = None):
+    """A raw DEFLATE stream from bit 0 to its final block (the decode of
+    decompress_raw_bytes, src/decompress/mod.rs:920), output capacity `cap`
+    bytes.  Returns (status, bytes or None, end bit)."""
+    a = _u8(data)
+    st, res, out = inflate_chunk(a, 0, cap=cap or max(1 << 16, a.size * 16))
+    ok = st == 0 and res.final_block
+    return (st if not ok else 0), (out.astype(np.uint8).tobytes() if ok else None), res.end_bit
+
+
 START_SYNC, ZERO_WINDOW = 1, 2
 
 
