@@ -122,6 +122,7 @@ def lib():
             L.gzgpu_decompress.argtypes = [vp, vp, sz, vp, sz, ctypes.POINTER(sz)]
             L.gzgpu_decompress_device.argtypes = [vp, vp, sz, vp, sz, ctypes.POINTER(sz)]
             L.gzgpu_inflate_raw.argtypes = [vp, vp, sz, vp, sz, ctypes.POINTER(sz)]
+            L.gzgpu_build_index.argtypes = [vp, vp, sz, ctypes.c_uint64, vp, sz, ctypes.POINTER(sz)]
             L.gzgpu_decompress_to_writer.argtypes = [vp, vp, sz, WRITE_FN, vp,
                                                      ctypes.POINTER(ctypes.c_uint64)]
             u64p = ctypes.POINTER(ctypes.c_uint64)
@@ -241,6 +242,28 @@ class Context:
             n = ctypes.c_size_t(0)
             rc = self._lib.gzgpu_inflate_raw(self._h, a.ctypes.data, a.size, out.ctypes.data, cap,
                                              ctypes.byref(n))
+            if rc == OUT_TOO_SMALL:
+                cap = n.value
+                continue
+            if rc != OK:
+                _raise(rc)
+            return out[:n.value].tobytes()
+        _raise(OUT_TOO_SMALL)
+
+    def build_index(self, data, interval_bytes: int = 1 << 20) -> bytes:
+        """gzippy's seek index of a single-member gzip buffer (build_index +
+        serialize_index, src/decompress/index.rs:55-141), version 1 layout.
+        Sized from the member's ISIZE; a short guess (ISIZE wraps past
+        4 GiB) is retried at the exact size."""
+        a = _as_u8(data)
+        isize = int(a[-4:].view("<u4")[0]) if a.size >= 4 else 0
+        pts = isize // max(interval_bytes, 1) + 2 if interval_bytes else isize // 1024 + 2
+        cap = 24 + pts * (16 + 32768)
+        for _ in range(2):
+            out = np.empty(cap, dtype=np.uint8)
+            n = ctypes.c_size_t(0)
+            rc = self._lib.gzgpu_build_index(self._h, a.ctypes.data, a.size, interval_bytes,
+                                             out.ctypes.data, cap, ctypes.byref(n))
             if rc == OUT_TOO_SMALL:
                 cap = n.value
                 continue
@@ -434,6 +457,26 @@ def decompress_raw(data) -> bytes:
 
 
 deflate_decode = decompress_raw  # the reference's alias (src/lib.rs:258)
+
+
+def build_index(data, interval_bytes: int = 1 << 20) -> bytes:
+    """gzippy's seek index of a single-member gzip buffer (index.rs:55)."""
+    return _ctx().build_index(data, interval_bytes)
+
+
+def parse_index(blob: bytes):
+    """(deflate offset, output size, [(bit offset, output offset, window)])
+    of a version 1 index (load_index, src/decompress/index.rs:185-290)."""
+    import struct
+    if blob[:6] != b"GZIDX\x01":
+        raise GzippyError("Parse", "not a version 1 seek index")
+    doff, total, n, _ = struct.unpack_from("<IQIH", blob, 6)
+    pts, at = [], 24
+    for _ in range(n):
+        b, o = struct.unpack_from("<QQ", blob, at)
+        pts.append((b, o, blob[at + 16:at + 16 + 32768]))
+        at += 16 + 32768
+    return doff, total, pts
 
 
 def decompress_to_writer(data, writer) -> int:

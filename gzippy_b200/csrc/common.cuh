@@ -100,12 +100,24 @@ constexpr uint32_t kSeqMask = 0x00FFFFFFu;
 constexpr int kGenShift = 24;
 constexpr uint32_t kMaxTries = 4;  // speculative starts tried per chunk
 
+// one DEFLATE block a chunk decoded (seek-index builds only): where its
+// header starts and how much output the chunk had produced before it
+struct BlockRec {
+  uint64_t hdr_bit;  // absolute input bit of the block header
+  uint64_t out_pos;  // chunk-local output position at the block's start
+  uint32_t chunk, gen;
+};
+
 struct PagePool {
   uint16_t* data;    // cap * kPageEntries entries
   uint32_t* owner;   // chunk id per page
   uint32_t* seq;     // page index within its chunk
   uint32_t* next;    // allocation counter
   uint32_t cap;
+  // block log: null unless a seek index is being built
+  BlockRec* blocks = nullptr;
+  uint32_t* n_blocks = nullptr;
+  uint32_t blocks_cap = 0;
 };
 
 // resolve plan entry: one accepted chunk in output order

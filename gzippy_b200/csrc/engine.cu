@@ -179,11 +179,19 @@ struct gzgpu_ctx {
   DevBuf in, out, s_off, s_len, info, units, cands, counters, descs, results, spec, work;
   DevBuf pages, owner, seq, placed, placed_of, list, segs, cblocks, bcrcs, mblk, mtrail, mlen,
       mcrc, mstatus;
+  // seek-index builds: the decoder's block log, the checkpoint interval and
+  // the serialized index of the last job (gzgpu_build_index)
+  DevBuf blk_log;
+  uint32_t blk_cap = 0, blk_need = 0;
+  bool job_index = false;
+  uint64_t index_interval = 0;
+  int index_status = 0;
+  std::vector<uint8_t> index_bytes;
   HostPinned h_stage;
   std::vector<DevBuf*> all_bufs() {
     return {&in,     &out,   &s_off,   &s_len,  &info,   &units,   &cands,  &counters, &descs,
             &results, &spec, &work,    &pages,  &owner,  &seq,     &placed, &placed_of, &list,
-            &segs,   &cblocks, &bcrcs, &mblk,   &mtrail, &mlen,    &mcrc,   &mstatus};
+            &segs,   &cblocks, &bcrcs, &mblk,   &mtrail, &mlen,    &mcrc,   &mstatus, &blk_log};
   }
   const uint8_t* cur_in = nullptr;  // input buffer of the running job
   uint8_t* user_out = nullptr;       // caller device output (device-resident API)
@@ -202,6 +210,11 @@ struct gzgpu_ctx {
     PagePool pool{pages.as<uint16_t>(), owner.as<uint32_t>(), seq.as<uint32_t>(),
                   counters.as<uint32_t>() + 2, (uint32_t)(pages.cap / (kPageEntries * 2))};
     pool.cap = (uint32_t)std::min<uint64_t>(pool.cap, std::min(owner.cap, seq.cap) / 4);
+    if (job_index) {
+      pool.blocks = blk_log.as<BlockRec>();
+      pool.n_blocks = counters.as<uint32_t>() + 8;
+      pool.blocks_cap = blk_cap;
+    }
     cudaError_t e = cudaMemsetAsync(counters.as<uint32_t>() + 3, 0, 4, st);
     if (e != cudaSuccess) return e;
     stats.kernel_launches++;
@@ -626,6 +639,13 @@ int gzgpu_ctx::run(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R) 
         (rc = check(owner.ensure(4 * pages_needed))) || (rc = check(seq.ensure(4 * pages_needed))))
       return rc;
     cudaMemsetAsync(counters.as<uint32_t>() + 2, 0, 4, st);
+    if (job_index) {
+      // the block log restarts with every full decode pass
+      blk_cap = (uint32_t)std::min<uint64_t>(std::max<uint64_t>(blk_need, total_in / 64 + 65536),
+                                             1u << 30);
+      if ((rc = check(blk_log.ensure(sizeof(BlockRec) * (uint64_t)blk_cap)))) return rc;
+      cudaMemsetAsync(counters.as<uint32_t>() + 8, 0, 4, st);
+    }
     cudaEventRecord(ev[8], st);
     if ((rc = check(launch_decode(counters.as<uint32_t>() + 1)))) return rc;
     cudaEventRecord(ev[9], st);
@@ -1077,6 +1097,94 @@ int gzgpu_ctx::run(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R) 
         if (R[s].status == kOk && mst[mi] != kOk) R[s].status = mst[mi];
     }
   }
+  if (job_index) {
+    // seek index (build_index / scan_deflate, src/decompress/index.rs:55-141,
+    // src/decompress/scan_inflate.rs:46-130): walk the blocks of the one
+    // member in output order; at a block start whose output offset has
+    // reached the next checkpoint (and at least one window), record the
+    // header's bit (from the deflate start), the offset and the 32 KiB of
+    // output before it
+    index_bytes.clear();
+    index_status = kOk;
+    size_t n_mem = 0;
+    if (ns == 1)
+      for (const Walker& w : SW[0]) n_mem += w.members.size();
+    if (ns != 1 || R[0].status != kOk || n_mem != 1) {
+      index_status = ns == 1 && R[0].status != kOk ? R[0].status : GZGPU_INVALID_ARGUMENT;
+    } else {
+      uint32_t nrec = 0;
+      if ((rc = check(cudaMemcpyAsync(&nrec, counters.as<uint32_t>() + 8, 4, cudaMemcpyDeviceToHost, st))) ||
+          (rc = check(cudaStreamSynchronize(st))))
+        return rc;
+      if (nrec > blk_cap) {
+        blk_need = nrec + nrec / 4 + 1024;  // the caller decodes again with a larger log
+        index_status = kPoolExhausted;
+      } else {
+        std::vector<BlockRec> recs(nrec);
+        if (nrec && ((rc = check(cudaMemcpyAsync(recs.data(), blk_log.p, sizeof(BlockRec) * nrec,
+                                                 cudaMemcpyDeviceToHost, st))) ||
+                     (rc = check(cudaStreamSynchronize(st)))))
+          return rc;
+        std::sort(recs.begin(), recs.end(), [](const BlockRec& a, const BlockRec& b) {
+          return a.chunk != b.chunk ? a.chunk < b.chunk : a.hdr_bit < b.hdr_bit;
+        });
+        const uint64_t deflate_bit = (S[0].off + hinfo[0].header_len) * 8;
+        const uint64_t interval = index_interval;
+        uint64_t next_cp = interval;
+        std::vector<std::pair<uint64_t, uint64_t>> pts;  // (bit from the deflate start, output offset)
+        uint64_t prev_end = kNoStop;
+        for (const PlacedChunk& p : placed) {
+          const uint32_t cid = p.chunk;
+          auto it = std::lower_bound(recs.begin(), recs.end(), cid,
+                                     [](const BlockRec& a, uint32_t c) { return a.chunk < c; });
+          uint64_t last_bit = kNoStop;
+          for (; it != recs.end() && it->chunk == cid; ++it) {
+            // the accepted attempt's blocks inside its decoded range, once each
+            if (it->gen != hr[cid].gen || it->hdr_bit < hd[cid].start_bit || it->hdr_bit >= hr[cid].end_bit ||
+                it->hdr_bit == last_bit)
+              continue;
+            last_bit = it->hdr_bit;
+            // a chunk accepted from a start range (a stored block's header
+            // and padding bits) began where its predecessor ended: that bit
+            // is the block's boundary in the stream
+            uint64_t bit = it->hdr_bit;
+            if (bit == hd[cid].start_bit && !(hd[cid].flags & kChunkMemberFirst) && prev_end != kNoStop)
+              bit = prev_end;
+            const uint64_t out = p.out_off - R[0].out_off + it->out_pos;
+            if (out >= next_cp && out >= kWindow) {
+              pts.emplace_back(bit - deflate_bit, out);
+              next_cp = out + interval;
+            }
+          }
+          prev_end = hr[cid].end_bit;
+        }
+        const bool none = pts.empty();
+        if (none) pts.emplace_back(0, 0);  // one point at the start (index.rs:124-134)
+        constexpr size_t kPoint = 8 + 8 + kWindow;
+        index_bytes.assign(6 + 4 + 8 + 4 + 2 + pts.size() * kPoint, 0);
+        uint8_t* q = index_bytes.data();
+        auto put = [&](uint64_t v, int n) {
+          for (int i = 0; i < n; i++) *q++ = (uint8_t)(v >> (8 * i));
+        };
+        memcpy(q, "GZIDX\x01", 6);
+        q += 6;
+        put(hinfo[0].header_len, 4);
+        put(R[0].out_len, 8);
+        put(pts.size(), 4);
+        put(0, 2);
+        for (const auto& pt : pts) {
+          put(pt.first, 8);
+          put(pt.second, 8);
+          if (!none &&
+              (rc = check(cudaMemcpyAsync(q, cur_out + R[0].out_off + pt.second - kWindow, kWindow,
+                                          cudaMemcpyDeviceToHost, st))))
+            return rc;
+          q += kWindow;
+        }
+        if ((rc = check(cudaStreamSynchronize(st)))) return rc;
+      }
+    }
+  }
   float t;
   auto el = [&](int a, int b) {
     t = 0;
@@ -1246,6 +1354,50 @@ int gzgpu_inflate_raw(gzgpu_ctx* c, const uint8_t* in, size_t in_len, uint8_t* o
   const int rc = decompress_host(c, in, in_len, out, out_cap, out_len);
   c->job_raw = false;
   return rc;
+}
+
+int gzgpu_build_index(gzgpu_ctx* c, const uint8_t* in, size_t in_len, uint64_t interval_bytes,
+                      uint8_t* index_out, size_t index_cap, size_t* index_len) {
+  if (!c || !index_len || (!in && in_len) || (!index_out && index_cap)) return GZGPU_INVALID_ARGUMENT;
+  *index_len = 0;
+  // build_index (src/decompress/index.rs:55-80): gzip only, one member, and
+  // not gzippy's multi-block format (its blocks are their own index)
+  if (in_len < 18 || in[0] != 0x1f || in[1] != 0x8b) return GZGPU_INVALID_ARGUMENT;
+  if (in[3] & 4) {
+    const size_t xlen = in[10] | (in[11] << 8);
+    for (size_t p = 12; p + 4 <= 12 + xlen && 12 + xlen <= in_len;) {
+      if (in[p] == 'G' && in[p + 1] == 'Z') return GZGPU_INVALID_ARGUMENT;
+      p += 4 + (in[p + 2] | (in[p + 3] << 8));
+    }
+  }
+  std::lock_guard<std::mutex> g(c->mu);
+  cudaSetDevice(c->dev);
+  int rc;
+  if ((rc = c->check(c->in.ensure(in_len + kInputPad)))) return rc;
+  c->job_index = true;
+  c->index_interval = interval_bytes;
+  c->blk_need = 0;
+  for (int attempt = 0; attempt < 2; attempt++) {
+    reset_stats(c);
+    cudaEventRecord(c->ev[0], c->st);
+    if ((rc = stage_input(c, in, in_len, 0))) break;
+    cudaMemsetAsync(c->in.as<uint8_t>() + in_len, 0, kInputPad, c->st);
+    c->cur_in = c->in.as<uint8_t>();
+    c->user_out = nullptr;
+    std::vector<StreamSpec> S{{0, in_len}};
+    std::vector<StreamOut> R;
+    rc = c->job(S, R);
+    if (rc != kOk) break;
+    finish_stats(c);
+    rc = c->index_status;
+    if (rc != kPoolExhausted || !c->blk_need) break;  // else: again with the log sized to fit
+  }
+  c->job_index = false;
+  if (rc != kOk) return rc == kPoolExhausted ? GZGPU_DEVICE_ERROR : rc;
+  *index_len = c->index_bytes.size();
+  if (c->index_bytes.size() > index_cap) return GZGPU_OUT_TOO_SMALL;
+  memcpy(index_out, c->index_bytes.data(), c->index_bytes.size());
+  return GZGPU_OK;
 }
 
 int gzgpu_decompress_device(gzgpu_ctx* c, const void* d_in, size_t in_len, void* d_out,

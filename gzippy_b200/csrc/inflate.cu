@@ -914,6 +914,10 @@ __device__ int32_t decode_chunk(const uint8_t* __restrict__ in, ChunkDesc d,
       }
     } else {
       blk_hdr = bitpos;
+      if (pool.blocks && lane == 0) {
+        const uint32_t k = atomicAdd(pool.n_blocks, 1u);
+        if (k < pool.blocks_cap) pool.blocks[k] = BlockRec{bitpos, o, cid, gen};
+      }
       br.refill(lane);
       const uint32_t hdr = (uint32_t)br.bb & 7;
       br.consume(3);

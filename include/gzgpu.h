@@ -118,6 +118,19 @@ int gzgpu_decompress(gzgpu_ctx *ctx, const uint8_t *in, size_t in_len, uint8_t *
 int gzgpu_inflate_raw(gzgpu_ctx *ctx, const uint8_t *in, size_t in_len, uint8_t *out,
                       size_t out_cap, size_t *out_len);
 
+/* gzippy's seek index (build_index + serialize_index, src/decompress/index.rs:
+ * 55-141; checkpoint rule of scan_deflate, src/decompress/scan_inflate.rs:
+ * 46-130), built from the parallel decode: at each DEFLATE block start whose
+ * output offset has reached the next checkpoint (interval_bytes after the
+ * previous one) and at least 32 KiB, a point records the header's bit offset
+ * from the deflate start, the output offset and the 32 KiB of output before
+ * it.  Written in the index format's version 1 layout ("GZIDX\x01", the
+ * layout load_index reads with a bit offset per point).  Single-member gzip
+ * only: other input gives GZGPU_INVALID_ARGUMENT, as in the reference.  On
+ * GZGPU_OUT_TOO_SMALL *index_len is the size needed. */
+int gzgpu_build_index(gzgpu_ctx *ctx, const uint8_t *in, size_t in_len, uint64_t interval_bytes,
+                      uint8_t *index_out, size_t index_cap, size_t *index_len);
+
 /* gzippy::decompress_to_writer / _with_threads (src/lib.rs:204,221):
  * output delivered in order through `write` (return 0 to continue, non-zero
  * to abort with GZGPU_INVALID_ARGUMENT); *written = total bytes delivered. */

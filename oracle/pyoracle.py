@@ -156,6 +156,54 @@ def inflate_raw(data, cap: int | None = None):
     return (st if not ok else 0), (out.astype(np.uint8).tobytes() if ok else None), res.end_bit
 
 
+def block_starts(data, plain_len: int):
+    """Every DEFLATE block of the single member `data` in stream order, as
+    (absolute header bit, output offset at the block's start), by decoding
+    one block at a time with the previous 32 KiB as window (the loop of
+    scan_deflate, src/decompress/scan_inflate.rs:63-124).  plain_len is the
+    member's output size."""
+    a = _u8(data)
+    st, hl = gzip_header_len(a)
+    assert st == 0
+    bit, out, win, blocks = hl * 8, 0, b"", []
+    while True:
+        blocks.append((bit, out))
+        cap = min(plain_len - out + 64, 8 << 20)
+        st, res, ent = inflate_chunk(a, bit, stop_lo=bit + 1, window=win, cap=cap)
+        assert st == 0, st
+        chunk = ent.astype(np.uint8).tobytes()
+        win = (win + chunk)[-32768:]
+        out += len(chunk)
+        bit = res.end_bit
+        if res.final_block:
+            return blocks
+
+
+def seek_index(data, plain: bytes, interval: int) -> bytes:
+    """The seek index of a single-member gzip `data` whose output is `plain`:
+    the checkpoint rule of scan_deflate (src/decompress/scan_inflate.rs:65-76)
+    over block_starts, serialized in the version 1 layout load_index reads
+    (src/decompress/index.rs:185-290): "GZIDX\\x01", deflate offset u32,
+    output size u64, point count u32, 2 reserved bytes, then per point the
+    bit offset from the deflate start u64, the output offset u64 and the
+    32 KiB window.  No point qualifying gives one point at the start with a
+    zero window (index.rs:124-134)."""
+    import struct
+    _, hl = gzip_header_len(data)
+    pts, nxt = [], interval
+    for bit, out in block_starts(data, len(plain)):
+        if out >= nxt and out >= 32768:
+            pts.append((bit - hl * 8, out))
+            nxt = out + interval
+    body = []
+    if not pts:
+        body.append(struct.pack("<QQ", 0, 0) + bytes(32768))
+    for b, o in pts:
+        body.append(struct.pack("<QQ", b, o) + plain[o - 32768:o])
+    return (b"GZIDX\x01" + struct.pack("<IQIH", hl, len(plain), max(1, len(pts)), 0)
+            + b"".join(body))
+
+
 START_SYNC, ZERO_WINDOW = 1, 2
 
 
