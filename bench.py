@@ -66,6 +66,11 @@ def load_workload(name: str, scale: float):
     if name == "single_member_mixed":
         segs = max(4, int(round(256 * scale)))
         wl = W.single_member_mixed(segments=segs, keep_plain=True)
+    elif name == "stored_member":
+        # the same 1 GiB of mixed content at level 0: a member of stored
+        # blocks only (the stored-dominated case of stored_split.rs)
+        segs = max(4, int(round(256 * scale)))
+        wl = W.single_member_mixed(segments=segs, keep_plain=True, level=0)
     elif name == "single_member_text":
         wl = W.single_member_text(size=max(1 << 20, int((64 << 20) * scale)), keep_plain=True)
     elif name == "multi_member":

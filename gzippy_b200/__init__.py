@@ -122,6 +122,7 @@ def lib():
             L.gzgpu_decompress.argtypes = [vp, vp, sz, vp, sz, ctypes.POINTER(sz)]
             L.gzgpu_decompress_device.argtypes = [vp, vp, sz, vp, sz, ctypes.POINTER(sz)]
             L.gzgpu_inflate_raw.argtypes = [vp, vp, sz, vp, sz, ctypes.POINTER(sz)]
+            L.gzgpu_inflate_zlib.argtypes = [vp, vp, sz, vp, sz, ctypes.POINTER(sz)]
             L.gzgpu_build_index.argtypes = [vp, vp, sz, ctypes.c_uint64, vp, sz, ctypes.POINTER(sz)]
             L.gzgpu_decompress_to_writer.argtypes = [vp, vp, sz, WRITE_FN, vp,
                                                      ctypes.POINTER(ctypes.c_uint64)]
@@ -229,7 +230,7 @@ class Context:
             return out[:n.value].tobytes()
         _raise(OUT_TOO_SMALL)
 
-    def inflate_raw(self, data) -> bytes:
+    def inflate_raw(self, data, _entry: str = "gzgpu_inflate_raw") -> bytes:
         """One raw DEFLATE stream (gzippy::decompress_raw, src/lib.rs:250):
         decoded up to its final block, trailing bytes ignored; raises on
         invalid or cut-off data.  The first output guess is 4x the input, as
@@ -237,11 +238,11 @@ class Context:
         retried once at the exact size."""
         a = _as_u8(data)
         cap = max(4096, a.size * 4)
+        fn = getattr(self._lib, _entry)
         for _ in range(2):
             out = np.empty(cap, dtype=np.uint8)
             n = ctypes.c_size_t(0)
-            rc = self._lib.gzgpu_inflate_raw(self._h, a.ctypes.data, a.size, out.ctypes.data, cap,
-                                             ctypes.byref(n))
+            rc = fn(self._h, a.ctypes.data, a.size, out.ctypes.data, cap, ctypes.byref(n))
             if rc == OUT_TOO_SMALL:
                 cap = n.value
                 continue
@@ -249,6 +250,14 @@ class Context:
                 _raise(rc)
             return out[:n.value].tobytes()
         _raise(OUT_TOO_SMALL)
+
+    def inflate_zlib(self, data) -> bytes:
+        """zlib data (decompress_zlib_turbo, src/decompress/mod.rs:895): the
+        DEFLATE stream between the 2-byte header and the Adler-32 trailer,
+        neither checked, as in the reference."""
+        if len(data) < 6:
+            _raise(INVALID_ARGUMENT)
+        return self.inflate_raw(data, "gzgpu_inflate_zlib")
 
     def build_index(self, data, interval_bytes: int = 1 << 20) -> bytes:
         """gzippy's seek index of a single-member gzip buffer (build_index +
@@ -457,6 +466,11 @@ def decompress_raw(data) -> bytes:
 
 
 deflate_decode = decompress_raw  # the reference's alias (src/lib.rs:258)
+
+
+def decompress_zlib(data) -> bytes:
+    """zlib data (decompress_zlib_turbo, src/decompress/mod.rs:895)."""
+    return _ctx().inflate_zlib(data)
 
 
 def build_index(data, interval_bytes: int = 1 << 20) -> bytes:

@@ -1356,6 +1356,16 @@ int gzgpu_inflate_raw(gzgpu_ctx* c, const uint8_t* in, size_t in_len, uint8_t* o
   return rc;
 }
 
+int gzgpu_inflate_zlib(gzgpu_ctx* c, const uint8_t* in, size_t in_len, uint8_t* out,
+                       size_t out_cap, size_t* out_len) {
+  if (!c || !out_len || (!in && in_len) || (!out && out_cap)) return GZGPU_INVALID_ARGUMENT;
+  *out_len = 0;
+  // decompress_zlib_turbo (src/decompress/mod.rs:895-914): the DEFLATE data
+  // between the 2-byte header and the 4-byte Adler-32, neither checked
+  if (in_len < 6) return GZGPU_INVALID_ARGUMENT;
+  return gzgpu_inflate_raw(c, in + 2, in_len - 6, out, out_cap, out_len);
+}
+
 int gzgpu_build_index(gzgpu_ctx* c, const uint8_t* in, size_t in_len, uint64_t interval_bytes,
                       uint8_t* index_out, size_t index_cap, size_t* index_len) {
   if (!c || !index_len || (!in && in_len) || (!index_out && index_cap)) return GZGPU_INVALID_ARGUMENT;

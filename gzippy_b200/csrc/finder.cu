@@ -15,7 +15,8 @@ namespace gzgpu {
 // [guess_bit, limit_bit) round-robin, each window searched for its first
 // candidate (by start bit, so windows partition the candidates); a warp stops
 // as soon as a lower window has a hit, so the work is about the distance to
-// the first candidate, split over the CTA's warps.
+// the first candidate, split over the CTA's warps.  Stored candidates must
+// also pass start_ok (a stored or dynamic block right after them).
 constexpr int kFinderWarps = 8;
 constexpr uint64_t kFinderWindow = 1024;
 
@@ -39,8 +40,16 @@ __global__ void __launch_bounds__(32 * kFinderWarps)
     if (k > *(volatile unsigned long long*)&best_win) break;
     const uint64_t w0 = from + k * kFinderWindow;
     const uint64_t w1 = min(w0 + kFinderWindow, to);
-    uint64_t lo = 0, hi = 0;
-    if (warp_find_first(in, nbytes, w0, w1, to, lane, lo, hi, leaf_lut)) {
+    uint64_t lo = 0, hi = 0, s0 = w0;
+    bool hit = false;
+    while (s0 < w1 && warp_find_first(in, nbytes, s0, w1, to, lane, lo, hi, leaf_lut)) {
+      if (start_ok(in, nbytes, hi)) {
+        hit = true;
+        break;
+      }
+      s0 = lo + 1;  // a stored match without a plausible successor
+    }
+    if (hit) {
       if (lane == 0) {
         hit_lo[warp] = lo;
         hit_hi[warp] = hi;

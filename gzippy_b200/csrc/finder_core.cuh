@@ -209,6 +209,42 @@ static __device__ __forceinline__ bool dyn_candidate_fast(const uint8_t* in, uin
   return dyn_candidate_full(in, nbytes, bit);
 }
 
+// The block after a true non-final stored block starts at byte `n` (its
+// header's first bit is bit 0 of that byte): another stored block (LEN ==
+// ~NLEN one byte on) or a dynamic block whose header passes the full
+// predicate.  Not a rule of the reference's finder: it drops the false
+// LEN/NLEN matches (about one per 64 KiB of random bytes) that would
+// otherwise start speculative chunks inside stored data.  A true stored
+// block followed by a fixed-Huffman block is given up as a start.
+static __device__ __forceinline__ bool stored_successor_ok(const uint8_t* in, uint64_t nbytes,
+                                                           uint64_t n) {
+  if (n >= nbytes) return false;
+  const uint32_t bt = (in[n] >> 1) & 3;
+  if (bt == 0) {
+    if (n + 5 > nbytes) return false;
+    const uint32_t sz = in[n + 1] | (in[n + 2] << 8) | ((uint32_t)in[n + 3] << 16) |
+                        ((uint32_t)in[n + 4] << 24);
+    return ((sz ^ (sz >> 16)) & 0xFFFF) == 0xFFFF;
+  }
+  if (bt != 2) return false;
+  const uint64_t bit = n * 8;
+  if (bit + 17 > nbytes * 8) return false;
+  const uint32_t h = (uint32_t)peek_bits(in, nbytes, bit, 13);
+  if (((h >> 3) & 31) > 29 || ((h >> 8) & 31) > 29) return false;
+  return dyn_candidate_full(in, nbytes, bit);
+}
+
+// A candidate found at seek bit `hi` stays a chunk start unless it is a stored
+// block whose successor fails stored_successor_ok (the finder kernel then
+// searches on from its first bit + 1; the decoder's in-kernel retry takes
+// the reference's candidates as they are).
+static __device__ __forceinline__ bool start_ok(const uint8_t* in, uint64_t nbytes, uint64_t hi) {
+  if (((peek_bits(in, nbytes, hi, 3) >> 1) & 3) != 0) return true;
+  const uint64_t off = (hi + 3) >> 3;
+  const uint32_t len = in[off] | (in[off + 1] << 8);
+  return stored_successor_ok(in, nbytes, off + 4 + len);
+}
+
 // Stored candidate test at byte offset `off` (find_uncompressed_blocks):
 // LEN == ~NLEN at the byte boundary, 3 zero header bits before it; the
 // candidate spans [byte_bit - zero_run, byte_bit - 3].

@@ -118,6 +118,13 @@ int gzgpu_decompress(gzgpu_ctx *ctx, const uint8_t *in, size_t in_len, uint8_t *
 int gzgpu_inflate_raw(gzgpu_ctx *ctx, const uint8_t *in, size_t in_len, uint8_t *out,
                       size_t out_cap, size_t *out_len);
 
+/* decompress_zlib_turbo (src/decompress/mod.rs:895-914): zlib data decoded
+ * as the raw DEFLATE stream between its 2-byte header and 4-byte Adler-32
+ * trailer; like the reference, neither is checked.  Fewer than 6 bytes:
+ * GZGPU_INVALID_ARGUMENT; otherwise as gzgpu_inflate_raw. */
+int gzgpu_inflate_zlib(gzgpu_ctx *ctx, const uint8_t *in, size_t in_len, uint8_t *out,
+                       size_t out_cap, size_t *out_len);
+
 /* gzippy's seek index (build_index + serialize_index, src/decompress/index.rs:
  * 55-141; checkpoint rule of scan_deflate, src/decompress/scan_inflate.rs:
  * 46-130), built from the parallel decode: at each DEFLATE block start whose

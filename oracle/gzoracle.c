@@ -725,11 +725,13 @@ static int lengths_complete(const uint8_t *l, int n) {
   return leaves == (1u << 15);
 }
 
-static int dyn_candidate(const uint8_t *data, size_t n, uint64_t bit) {
+/* any_final: accept BFINAL = 1 too (the header of a block that follows a
+ * stored candidate, stored_successor_ok) */
+static int dyn_candidate_h(const uint8_t *data, size_t n, uint64_t bit, int any_final) {
   uint64_t nbits = (uint64_t)n * 8;
   if (bit + 17 > nbits) return 0;
   uint32_t h = (uint32_t)bits_at(data, n, bit, 17);
-  if (!hdr_filter(h, 13)) return 0;
+  if (!hdr_filter(any_final ? h & ~1u : h, 13)) return 0;
   int hlit = (h >> 3) & 31, hdist = (h >> 8) & 31, hclen = (h >> 13) & 15;
   int pc = hclen + 4;
   if (bit + 17 + 3 * pc > nbits) return 0;
@@ -777,6 +779,27 @@ static int dyn_candidate(const uint8_t *data, size_t n, uint64_t bit) {
   return lengths_complete(lens, hl) && lengths_complete(lens + hl, total - hl);
 }
 
+static int dyn_candidate(const uint8_t *data, size_t n, uint64_t bit) {
+  return dyn_candidate_h(data, n, bit, 0);
+}
+
+/* The block after a true non-final stored block starts at byte nb: another
+ * stored block (LEN == ~NLEN one byte on) or a dynamic block passing the
+ * full header predicate.  The device's partition-start rule (finder_core.cuh
+ * stored_successor_ok), not the reference finder's: orc_find_blocks keeps
+ * the reference predicate, orc_find_starts adds this. */
+static int stored_successor_ok(const uint8_t *d, size_t n, uint64_t nb) {
+  if (nb >= n) return 0;
+  uint32_t bt = (d[nb] >> 1) & 3;
+  if (bt == 0) {
+    if (nb + 5 > n) return 0;
+    uint32_t sz = d[nb + 1] | (d[nb + 2] << 8) | ((uint32_t)d[nb + 3] << 16) |
+                  ((uint32_t)d[nb + 4] << 24);
+    return ((sz ^ (sz >> 16)) & 0xFFFF) == 0xFFFF;
+  }
+  return bt == 2 && dyn_candidate_h(d, n, nb * 8, 1);
+}
+
 int orc_is_dynamic_candidate(const uint8_t *data, size_t n, uint64_t bit) {
   return dyn_candidate(data, n, bit);
 }
@@ -793,7 +816,7 @@ static int cand_cmp(const void *a, const void *b) {
 }
 
 static size_t find_stored(const uint8_t *d, size_t n, uint64_t start_bit, uint64_t end_bit,
-                          cand_t *out, size_t cap) {
+                          cand_t *out, size_t cap, int succ) {
   size_t k = 0;
   if (n < 5) return 0;
   uint64_t until = (end_bit + 7) / 8;
@@ -816,6 +839,7 @@ static size_t find_stored(const uint8_t *d, size_t n, uint64_t start_bit, uint64
     if (earliest >= start_bit && latest < end_bit) {
       uint32_t len = sz & 0xFFFF;
       if (len == 0 || off + 4 + len > n) continue;
+      if (succ && !stored_successor_ok(d, n, off + 4 + len)) continue;
       if (k < cap) out[k] = (cand_t){earliest, latest};
       k++;
     }
@@ -823,8 +847,8 @@ static size_t find_stored(const uint8_t *d, size_t n, uint64_t start_bit, uint64
   return k;
 }
 
-size_t orc_find_blocks(const uint8_t *data, size_t n, uint64_t start_bit, uint64_t end_bit,
-                       uint64_t *first, uint64_t *seek, size_t cap) {
+static size_t find_blocks_impl(const uint8_t *data, size_t n, uint64_t start_bit, uint64_t end_bit,
+                               uint64_t *first, uint64_t *seek, size_t cap, int succ) {
   pthread_once(&skip_once, skip_init);
   uint64_t nbits = (uint64_t)n * 8;
   if (end_bit > nbits) end_bit = nbits;
@@ -844,10 +868,10 @@ size_t orc_find_blocks(const uint8_t *data, size_t n, uint64_t start_bit, uint64
     }
     p++;
   }
-  size_t ns = find_stored(data, n, start_bit, end_bit, NULL, 0);
+  size_t ns = find_stored(data, n, start_bit, end_bit, NULL, 0, succ);
   if (ns) {
     c = (cand_t *)realloc(c, (k + ns + 1) * sizeof(cand_t));
-    find_stored(data, n, start_bit, end_bit, c + k, ns);
+    find_stored(data, n, start_bit, end_bit, c + k, ns, succ);
     k += ns;
   }
   qsort(c, k, sizeof(cand_t), cand_cmp);
@@ -858,6 +882,16 @@ size_t orc_find_blocks(const uint8_t *data, size_t n, uint64_t start_bit, uint64
   }
   free(c);
   return k;
+}
+
+size_t orc_find_blocks(const uint8_t *data, size_t n, uint64_t start_bit, uint64_t end_bit,
+                       uint64_t *first, uint64_t *seek, size_t cap) {
+  return find_blocks_impl(data, n, start_bit, end_bit, first, seek, cap, 0);
+}
+
+size_t orc_find_starts(const uint8_t *data, size_t n, uint64_t start_bit, uint64_t end_bit,
+                       uint64_t *first, uint64_t *seek, size_t cap) {
+  return find_blocks_impl(data, n, start_bit, end_bit, first, seek, cap, 1);
 }
 
 /* first stored candidate (in byte order, hence smallest bit_offset) */
@@ -873,7 +907,7 @@ static int find_stored_first(const uint8_t *d, size_t n, uint64_t start_bit, uin
                   ((uint32_t)d[off + 3] << 24);
     if (((sz ^ (sz >> 16)) & 0xFFFF) != 0xFFFF) continue;
     cand_t c;
-    if (find_stored(d, n, start_bit, end_bit < off * 8 + 1 ? end_bit : off * 8 + 1, &c, 1) &&
+    if (find_stored(d, n, start_bit, end_bit < off * 8 + 1 ? end_bit : off * 8 + 1, &c, 1, 0) &&
         c.seek == off * 8 - 3) {
       *out = c;
       return 1;

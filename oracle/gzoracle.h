@@ -89,6 +89,10 @@ int orc_gzip_header(const uint8_t *p, size_t n, size_t *hdr_len);
  * sorted by (bit_offset, seek_bit).  Returns the number written (<= cap). */
 size_t orc_find_blocks(const uint8_t *data, size_t n, uint64_t start_bit, uint64_t end_bit,
                        uint64_t *first, uint64_t *seek, size_t cap);
+/* orc_find_blocks with the device's partition-start rule for stored
+ * candidates: the block after one must be stored or a valid dynamic block. */
+size_t orc_find_starts(const uint8_t *data, size_t n, uint64_t start_bit, uint64_t end_bit,
+                       uint64_t *first, uint64_t *seek, size_t cap);
 /* dynamic-header predicate at one bit offset (1 = candidate) */
 int orc_is_dynamic_candidate(const uint8_t *data, size_t n, uint64_t bit);
 

@@ -70,6 +70,8 @@ def lib():
             L.orc_gzip_header.argtypes = [vp, sz, ctypes.POINTER(sz)]
             L.orc_find_blocks.argtypes = [vp, sz, u64, u64, vp, vp, sz]
             L.orc_find_blocks.restype = sz
+            L.orc_find_starts.argtypes = [vp, sz, u64, u64, vp, vp, sz]
+            L.orc_find_starts.restype = sz
             L.orc_is_dynamic_candidate.argtypes = [vp, sz, u64]
             L.orc_inflate_chunk.argtypes = [vp, sz, u64, u64, ctypes.c_int, vp, sz, vp, sz,
                                             ctypes.POINTER(ChunkResult)]
@@ -117,6 +119,18 @@ def find_blocks(data, start_bit: int, end_bit: int, cap: int = 1 << 16):
     first = np.zeros(cap, np.uint64)
     seek = np.zeros(cap, np.uint64)
     k = lib().orc_find_blocks(a.ctypes.data, a.size, start_bit, end_bit,
+                              first.ctypes.data, seek.ctypes.data, cap)
+    k = min(k, cap)
+    return first[:k].copy(), seek[:k].copy()
+
+
+def find_starts(data, start_bit: int, end_bit: int, cap: int = 1 << 16):
+    """find_blocks with the device's partition-start rule for stored
+    candidates (the block after one is stored or a valid dynamic block)."""
+    a = _u8(data)
+    first = np.zeros(cap, np.uint64)
+    seek = np.zeros(cap, np.uint64)
+    k = lib().orc_find_starts(a.ctypes.data, a.size, start_bit, end_bit,
                               first.ctypes.data, seek.ctypes.data, cap)
     k = min(k, cap)
     return first[:k].copy(), seek[:k].copy()

@@ -46,11 +46,12 @@ def test_stream_matches_oracle_and_zlib(ctx, ctype, level):
 
 def _expected_start(data, f, t):
     """A partition's start: a sync start in fixed-Huffman data when there is
-    one (searched first), else the first block-start candidate."""
+    one (searched first), else the first block-start candidate (stored ones
+    need a stored or dynamic successor)."""
     b = O.fixed_sync_find(data, f, t)
     if b is not None:
         return ("sync", b)
-    first, seek = O.find_blocks(data, f, t, cap=1 << 18)
+    first, seek = O.find_starts(data, f, t, cap=1 << 18)
     return (int(first[0]), int(seek[0])) if first.size else None
 
 

@@ -86,3 +86,44 @@ def test_device_raw_errors():
         assert cx.inflate_raw(c) == p                    # the context still works
     finally:
         cx.close()
+
+
+@pytest.mark.gpu
+def test_device_zlib_matches_zlib():
+    """decompress_zlib_turbo (src/decompress/mod.rs:895-914): the DEFLATE data
+    between the 2-byte header and the Adler-32, neither checked."""
+    import gzippy_b200 as G
+    cx = G.Context()
+    try:
+        for kind, level, size in ((W.MARKOV, 6, 24 << 20), (W.RUNS, 9, 1 << 20), (W.RANDOM, 1, 64 << 10)):
+            p = W.content(kind, 730 + kind, size).tobytes()
+            z = zlib.compress(p, level)
+            assert cx.inflate_zlib(z) == p == zlib.decompress(z)
+        with pytest.raises(G.GzippyError):
+            cx.inflate_zlib(b"\x78\x9c\x03")                  # under 6 bytes
+    finally:
+        cx.close()
+
+
+def _stored_cases():
+    p = W.content(W.MARKOV, 740, 3 << 20).tobytes()
+    c = zlib.compressobj(6, zlib.DEFLATED, 31)
+    flushed = b"".join(c.compress(p[i:i + 1000]) + c.flush(zlib.Z_SYNC_FLUSH)
+                       for i in range(0, 200000, 1000)) + c.compress(p[200000:]) + c.flush()
+    mixed = b"".join(W.content(k % 4, 741 + k, 1 << 20).tobytes() for k in range(24))
+    return [("level0-mixed", mixed, W.gzip_member(np.frombuffer(mixed, np.uint8), 0).tobytes()),
+            ("empty-stored-blocks", p, flushed)]
+
+
+@pytest.mark.gpu
+def test_device_stored_members():
+    """Stored-only members (level 0, the stored-dominated case of
+    parallel/stored_split.rs) and members with hundreds of empty stored
+    blocks (sync flushes) decode byte-exact."""
+    import gzippy_b200 as G
+    cx = G.Context()
+    try:
+        for name, plain, comp in _stored_cases():
+            assert cx.decompress(comp) == plain == zlib.decompress(comp, 31), name
+    finally:
+        cx.close()
