@@ -20,6 +20,38 @@ namespace gzgpu {
 constexpr int kFinderWarps = 8;
 constexpr uint64_t kFinderWindow = 1024;
 
+// The first stored block start (by byte offset, hence by start bit) in the
+// sync-started chunk d's range whose successor passes stored_successor_ok
+// replaces the sync start.  All threads of the CTA scan 256 offsets a round;
+// `s_off` is CTA shared memory.
+static __device__ void sync_or_stored(const uint8_t* __restrict__ in, ChunkDesc& d,
+                                      unsigned long long* s_off) {
+  const uint64_t from = d.guess_bit, to = d.limit_bit, nbytes = d.in_end;
+  if (threadIdx.x == 0) *s_off = ~0ull;
+  __syncthreads();
+  const uint64_t until = nbytes >= 5 ? min((to + 7) / 8, nbytes - 4) : 0;
+  for (uint64_t base = max((from + 3 + 7) / 8, (uint64_t)2); base < until; base += blockDim.x) {
+    const uint64_t off = base + threadIdx.x;
+    uint64_t lo = 0, hi = 0;
+    if (off < until && stored_candidate(in, nbytes, off, from, to, to, lo, hi) &&
+        stored_successor_ok(in, nbytes, off + 4 + (in[off] | (in[off + 1] << 8))))
+      atomicMin(s_off, (unsigned long long)off);
+    __syncthreads();
+    const bool found = *s_off != ~0ull;
+    __syncthreads();  // every thread has read it before the next round writes
+    if (found) break;
+  }
+  if (threadIdx.x == 0 && *s_off != ~0ull) {
+    uint64_t lo = 0, hi = 0;
+    stored_candidate(in, nbytes, *s_off, from, to, to, lo, hi);
+    d.lo_bit = lo;
+    d.start_bit = hi;
+    d.flags &= ~kChunkSync;
+    d.table_bit = 0;
+    d.est_ratio = 1.f;
+  }
+}
+
 __global__ void __launch_bounds__(32 * kFinderWarps)
     finder_kernel(const uint8_t* __restrict__ in, ChunkDesc* descs,
                   const uint32_t* __restrict__ spec, uint32_t n_spec) {
@@ -29,7 +61,14 @@ __global__ void __launch_bounds__(32 * kFinderWarps)
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   if (blockIdx.x >= n_spec) return;
   ChunkDesc& d = descs[spec[blockIdx.x]];
-  if (d.flags & kChunkValid) return;  // a sync start was found first
+  if (d.flags & kChunkValid) {
+    // a sync start was found first.  It stands unless the partition holds a
+    // stored block start with a stored or dynamic successor: the raw bytes
+    // of stored blocks (text, runs) also walk as fixed-Huffman codes, so a
+    // sync start there is false, while such a stored start is real.
+    if (d.flags & kChunkSync) sync_or_stored(in, d, &best_win);
+    return;
+  }
   for (int i = threadIdx.x; i < 4096; i += blockDim.x) leaf_lut[i] = (uint16_t)precode_leaves4(i);
   const uint64_t from = d.guess_bit, to = d.limit_bit, nbytes = d.in_end;
   if (threadIdx.x == 0) best_win = ~0ull;

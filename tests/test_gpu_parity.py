@@ -46,12 +46,17 @@ def test_stream_matches_oracle_and_zlib(ctx, ctype, level):
 
 def _expected_start(data, f, t):
     """A partition's start: a sync start in fixed-Huffman data when there is
-    one (searched first), else the first block-start candidate (stored ones
-    need a stored or dynamic successor)."""
+    one (searched first) and the partition holds no stored block start, else
+    the first block-start candidate (stored ones need a stored or dynamic
+    successor)."""
+    first, seek = O.find_starts(data, f, t, cap=1 << 18)
     b = O.fixed_sync_find(data, f, t)
     if b is not None:
+        a = np.asarray(data, np.uint8)
+        for lo, hi in zip(first.tolist(), seek.tolist()):
+            if (int(a[hi // 8]) >> (hi % 8) | int(a[hi // 8 + 1]) << (8 - hi % 8)) >> 1 & 3 == 0:
+                return (int(lo), int(hi))          # a stored start replaces the sync start
         return ("sync", b)
-    first, seek = O.find_starts(data, f, t, cap=1 << 18)
     return (int(first[0]), int(seek[0])) if first.size else None
 
 
