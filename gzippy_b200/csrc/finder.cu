@@ -20,12 +20,24 @@ namespace gzgpu {
 constexpr int kFinderWarps = 8;
 constexpr uint64_t kFinderWindow = 1024;
 
-// The first stored block start (by byte offset, hence by start bit) in the
-// sync-started chunk d's range whose successor passes stored_successor_ok
-// replaces the sync start.  All threads of the CTA scan 256 offsets a round;
-// `s_off` is CTA shared memory.
-static __device__ void sync_or_stored(const uint8_t* __restrict__ in, ChunkDesc& d,
-                                      unsigned long long* s_off) {
+// Stored block starts, searched first for every speculative chunk: the first
+// one (by byte offset, hence by start bit) in [guess_bit, limit_bit) whose
+// successor passes stored_successor_ok becomes the chunk's start, and the
+// sync search and the block finder skip the chunk.  Such a start is real
+// (a false one needs two LEN/NLEN matches in a row, or a LEN/NLEN match and
+// a valid dynamic header), while the raw bytes of stored blocks (text, runs)
+// walk as fixed-Huffman codes and would give false sync starts.  One CTA of
+// kStoredThreads per chunk, scanning that many byte offsets a round.
+constexpr int kStoredThreads = 256;
+
+__global__ void __launch_bounds__(kStoredThreads)
+    stored_kernel(const uint8_t* __restrict__ in, ChunkDesc* descs,
+                  const uint32_t* __restrict__ spec, uint32_t n_spec) {
+  __shared__ unsigned long long s_first;
+  unsigned long long* s_off = &s_first;
+  if (blockIdx.x >= n_spec) return;
+  ChunkDesc& d = descs[spec[blockIdx.x]];
+  if (d.flags & kChunkValid) return;
   const uint64_t from = d.guess_bit, to = d.limit_bit, nbytes = d.in_end;
   if (threadIdx.x == 0) *s_off = ~0ull;
   __syncthreads();
@@ -46,8 +58,7 @@ static __device__ void sync_or_stored(const uint8_t* __restrict__ in, ChunkDesc&
     stored_candidate(in, nbytes, *s_off, from, to, to, lo, hi);
     d.lo_bit = lo;
     d.start_bit = hi;
-    d.flags &= ~kChunkSync;
-    d.table_bit = 0;
+    d.flags |= kChunkValid;
     d.est_ratio = 1.f;
   }
 }
@@ -61,14 +72,7 @@ __global__ void __launch_bounds__(32 * kFinderWarps)
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   if (blockIdx.x >= n_spec) return;
   ChunkDesc& d = descs[spec[blockIdx.x]];
-  if (d.flags & kChunkValid) {
-    // a sync start was found first.  It stands unless the partition holds a
-    // stored block start with a stored or dynamic successor: the raw bytes
-    // of stored blocks (text, runs) also walk as fixed-Huffman codes, so a
-    // sync start there is false, while such a stored start is real.
-    if (d.flags & kChunkSync) sync_or_stored(in, d, &best_win);
-    return;
-  }
+  if (d.flags & kChunkValid) return;  // a stored or sync start was found first
   for (int i = threadIdx.x; i < 4096; i += blockDim.x) leaf_lut[i] = (uint16_t)precode_leaves4(i);
   const uint64_t from = d.guess_bit, to = d.limit_bit, nbytes = d.in_end;
   if (threadIdx.x == 0) best_win = ~0ull;
@@ -209,9 +213,11 @@ __global__ void link_kernel(ChunkDesc* descs, uint32_t n, uint32_t* work, uint32
 cudaError_t launch_finder(const uint8_t* in, ChunkDesc* descs, const uint32_t* spec,
                           uint32_t n_spec, uint32_t* n_sync, cudaStream_t stream) {
   if (n_spec == 0) return cudaSuccess;
-  // The fixed-code sync search first: it costs a fraction of a full scan,
-  // which a fixed-Huffman partition (no block header to find) would need,
-  // and it fails within a few dozen symbols on other data.
+  // Stored starts first (a byte scan), then the fixed-code sync search: it
+  // costs a fraction of a full scan, which a fixed-Huffman partition (no
+  // block header to find) would need, and it fails within a few dozen
+  // symbols on other data.
+  stored_kernel<<<n_spec, kStoredThreads, 0, stream>>>(in, descs, spec, n_spec);
   sync_kernel<<<n_spec, kSyncOffsets, 0, stream>>>(in, descs, spec, n_spec, n_sync);
   finder_kernel<<<n_spec, 32 * kFinderWarps, 0, stream>>>(in, descs, spec, n_spec);
   return cudaGetLastError();

@@ -45,17 +45,17 @@ def test_stream_matches_oracle_and_zlib(ctx, ctype, level):
 
 
 def _expected_start(data, f, t):
-    """A partition's start: a sync start in fixed-Huffman data when there is
-    one (searched first) and the partition holds no stored block start, else
-    the first block-start candidate (stored ones need a stored or dynamic
-    successor)."""
+    """A partition's start: its first stored block start whose successor is a
+    stored or dynamic block (searched first); else a sync start in
+    fixed-Huffman data (searched next); else the first block-start
+    candidate."""
     first, seek = O.find_starts(data, f, t, cap=1 << 18)
+    a = np.concatenate([np.asarray(data, np.uint8), np.zeros(2, np.uint8)])
+    for lo, hi in zip(first.tolist(), seek.tolist()):
+        if (int(a[hi // 8]) >> (hi % 8) | int(a[hi // 8 + 1]) << (8 - hi % 8)) >> 1 & 3 == 0:
+            return (int(lo), int(hi))              # BTYPE 00 at the start: stored
     b = O.fixed_sync_find(data, f, t)
     if b is not None:
-        a = np.asarray(data, np.uint8)
-        for lo, hi in zip(first.tolist(), seek.tolist()):
-            if (int(a[hi // 8]) >> (hi % 8) | int(a[hi // 8 + 1]) << (8 - hi % 8)) >> 1 & 3 == 0:
-                return (int(lo), int(hi))          # a stored start replaces the sync start
         return ("sync", b)
     return (int(first[0]), int(seek[0])) if first.size else None
 
