@@ -164,3 +164,44 @@ def test_stream_semantics():
     for blob in (c + c, c + b"trailing garbage bytes!!"):
         st, out, _ = O.decompress_chunked(blob, chunk_bytes=8192, threads=2)
         assert st == O.OK
+
+
+def test_find_starts_keeps_true_stored_starts():
+    """The partition-start rule (orc_find_starts): a stored candidate needs a
+    stored or dynamic block right after it.  Its candidates are a subset of
+    the reference's (orc_find_blocks), every true stored block start whose
+    successor is stored or dynamic stays, and the false LEN/NLEN matches
+    inside stored random bytes go."""
+    import numpy as np
+    from gzippy_b200 import workloads as W
+    p = np.concatenate([W.content(k % 4, 60 + k, 1 << 20) for k in range(4)])
+    for level in (0, 6):
+        c = W.gzip_member(p, level)
+        blocks = O.block_starts(c, p.size)
+        bits = [b for b, _ in blocks]
+        a = np.concatenate([c, np.zeros(2, np.uint8)])
+
+        def btype(bit):
+            return ((int(a[bit // 8]) >> (bit % 8) | int(a[bit // 8 + 1]) << (8 - bit % 8)) >> 1) & 3
+
+        _, hl = O.gzip_header_len(c)
+        f_all, s_all = O.find_blocks(c, hl * 8, c.size * 8, cap=1 << 20)
+        f_st, s_st = O.find_starts(c, hl * 8, c.size * 8, cap=1 << 20)
+        ref = set(zip(f_all.tolist(), s_all.tolist()))
+        got = set(zip(f_st.tolist(), s_st.tolist()))
+        assert got <= ref
+        true_set = set(bits)
+        for k in range(1, len(bits) - 1):
+            b = bits[k]
+            if btype(b) != 0 or btype(bits[k + 1]) not in (0, 2):
+                continue
+            bfinal = (int(a[b // 8]) >> (b % 8)) & 1
+            # a non-final stored block with a non-empty LEN is a candidate
+            off = (b + 3 + 7) // 8
+            length = int(a[off]) | int(a[off + 1]) << 8
+            if bfinal or length == 0:
+                continue
+            assert any(lo <= b <= hi for lo, hi in got), (level, b)
+        false_ref = [x for x in ref if not any(x[0] <= t <= x[1] for t in true_set)]
+        false_got = [x for x in got if not any(x[0] <= t <= x[1] for t in true_set)]
+        assert len(false_got) <= len(false_ref) and len(false_got) <= 1, (level, len(false_ref), len(false_got))
