@@ -882,7 +882,7 @@ int gzgpu_ctx::run(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R) 
     bool rewalk = false;
     for (uint32_t s = 0; s < ns; s++) {
       bool bad = false;
-      for (auto& w : SW[s])  // judged once its optimistic repairs are verified
+      for (auto& w : SW[s])  // decided once its optimistic repairs are verified
         bad |= w.handoff_bad && (w.assumed.empty() || w.assumed.back().repair < hd.size());
       if (bad) {
         SW[s].clear();
