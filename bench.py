@@ -56,23 +56,28 @@ def load_workload(name: str, scale: float):
     """(compressed uint8 array, plain size, plain sha256, meta) -- cached on disk."""
     from gzippy_b200 import workloads as W
     os.makedirs(CACHE, exist_ok=True)
-    key = f"{name}_{scale:g}"
+    key = f"{name}_{scale:g}_v2"
     path = os.path.join(CACHE, key + ".gz")
     meta_path = os.path.join(CACHE, key + ".json")
     if os.path.exists(path) and os.path.exists(meta_path):
         meta = json.load(open(meta_path))
         return np.fromfile(path, dtype=np.uint8), meta
     t0 = time.time()
-    if name == "single_member_mixed":
+    # single members are one serial zlib stream; the "_pigz" variants are
+    # the same content in pigz-style framing (a Z_SYNC_FLUSH seam per MiB)
+    enc = "pigz" if name.endswith("_pigz") else "zlib-serial"
+    base = name[:-5] if name.endswith("_pigz") else name
+    if base == "single_member_mixed":
         segs = max(4, int(round(256 * scale)))
-        wl = W.single_member_mixed(segments=segs, keep_plain=True)
-    elif name == "stored_member":
+        wl = W.single_member_mixed(segments=segs, keep_plain=True, encoder=enc)
+    elif base == "stored_member":
         # the same 1 GiB of mixed content at level 0: a member of stored
         # blocks only (the stored-dominated case of stored_split.rs)
         segs = max(4, int(round(256 * scale)))
-        wl = W.single_member_mixed(segments=segs, keep_plain=True, level=0)
-    elif name == "single_member_text":
-        wl = W.single_member_text(size=max(1 << 20, int((64 << 20) * scale)), keep_plain=True)
+        wl = W.single_member_mixed(segments=segs, keep_plain=True, level=0, encoder=enc)
+    elif base == "single_member_text":
+        wl = W.single_member_text(size=max(1 << 20, int((64 << 20) * scale)), keep_plain=True,
+                                  encoder=enc)
     elif name == "multi_member":
         wl = W.multi_member(members=max(8, int(2048 * scale)), keep_plain=True)
     else:
@@ -81,8 +86,10 @@ def load_workload(name: str, scale: float):
     plain = wl.plain[0]
     meta = {"name": name, "plain_bytes": int(plain.size), "comp_bytes": int(comp.size),
             "sha256": hashlib.sha256(plain.tobytes()).hexdigest(),
-            "gen_s": round(time.time() - t0, 2), "meta": {k: v for k, v in wl.meta.items()
-                                                          if not isinstance(v, list)}}
+            "gen_s": round(time.time() - t0, 2), "encoder": wl.meta.get("encoder", "zlib-serial"),
+            "meta": {k: v for k, v in wl.meta.items() if not isinstance(v, list)}}
+    if "member_comp_bytes" in wl.meta:
+        meta["member_comp_bytes"] = wl.meta["member_comp_bytes"]
     comp.tofile(path)
     json.dump(meta, open(meta_path, "w"))
     return comp, meta
@@ -612,7 +619,8 @@ def main():
         if rank != 0:
             return
         comp, meta = load_workload(args.workload, args.scale)
-        config.update(plain_bytes=meta["plain_bytes"], comp_bytes=meta["comp_bytes"])
+        config.update(plain_bytes=meta["plain_bytes"], comp_bytes=meta["comp_bytes"],
+                      encoder=meta.get("encoder", "zlib-serial"))
         th = cpus()
         from oracle import pyoracle as O
         cap = meta["plain_bytes"] + 4096
@@ -651,7 +659,8 @@ def main():
     torch.cuda.set_device(local)
     import gzippy_b200 as G
     comp, meta = load_workload(args.workload, args.scale)
-    config.update(plain_bytes=meta["plain_bytes"], comp_bytes=meta["comp_bytes"])
+    config.update(plain_bytes=meta["plain_bytes"], comp_bytes=meta["comp_bytes"],
+                      encoder=meta.get("encoder", "zlib-serial"))
     ctx = G.Context(device=local, chunk_bytes=args.chunk_bytes, lut_bits=args.lut_bits,
                     ctas_per_sm=args.ctas_per_sm)
 

@@ -1,8 +1,11 @@
 """Seeded synthetic gzip workloads (the five decompression configurations).
 
 Every workload is generated on the machine that runs it from a seed, so no
-data files travel.  Content types, the zlib encoder stand-in and the
-pigz-style framing of large single members are described in ``synth.c``.
+data files travel.  Content types and the zlib encoder stand-in are
+described in ``synth.c``.  Every member is one serial zlib deflate stream
+(``encoder="zlib-serial"``); the pigz-style framing (parallel pieces closed
+by Z_SYNC_FLUSH, which leaves an empty stored block every piece) is only
+used when a caller names it (``encoder="pigz"``).
 
 Configurations (sizes scale with ``scale`` for tests):
 
@@ -115,17 +118,32 @@ class Workload:
         return int(sum(self.plain_sizes))
 
 
+ENCODERS = ("zlib-serial", "pigz")
+
+
+def encode_member(plain: np.ndarray, level: int, encoder: str = "zlib-serial",
+                  threads: int | None = None) -> np.ndarray:
+    """One gzip member: one serial deflate stream ("zlib-serial"), or the
+    pigz-style framing of 1 MiB pieces on `threads` threads ("pigz")."""
+    if encoder == "zlib-serial":
+        return gzip_member(plain, level, 1)
+    if encoder == "pigz":
+        return gzip_member(plain, level, threads or _cpus())
+    raise ValueError(f"unknown encoder {encoder!r}")
+
+
 def single_member_text(seed: int = 1234, size: int = 64 << 20, level: int = 6,
-                       keep_plain: bool = False, threads: int | None = None) -> Workload:
+                       keep_plain: bool = False, threads: int | None = None,
+                       encoder: str = "zlib-serial") -> Workload:
     plain = content(MARKOV, seed, size)
-    comp = gzip_member(plain, level, threads or _cpus())
+    comp = encode_member(plain, level, encoder, threads)
     return Workload("single_member_text", [comp], [size], [plain] if keep_plain else [],
-                    {"level": level, "seed": seed})
+                    {"level": level, "seed": seed, "encoder": encoder})
 
 
 def single_member_mixed(seed: int = 1235, segments: int = 256, seg_bytes: int = SEG,
                         level: int = 6, keep_plain: bool = False,
-                        threads: int | None = None) -> Workload:
+                        threads: int | None = None, encoder: str = "zlib-serial") -> Workload:
     plain = np.empty(segments * seg_bytes, dtype=np.uint8)
     th = threads or _cpus()
 
@@ -134,9 +152,10 @@ def single_member_mixed(seed: int = 1235, segments: int = 256, seg_bytes: int = 
 
     with ThreadPoolExecutor(th) as ex:
         list(ex.map(one, range(segments)))
-    comp = gzip_member(plain, level, th)
+    comp = encode_member(plain, level, encoder, th)
     return Workload("single_member_mixed", [comp], [plain.size], [plain] if keep_plain else [],
-                    {"level": level, "seed": seed, "segments": segments, "seg_bytes": seg_bytes})
+                    {"level": level, "seed": seed, "segments": segments, "seg_bytes": seg_bytes,
+                     "encoder": encoder})
 
 
 def multi_member(seed: int = 1236, members: int = 2048, member_bytes: int = 2 << 20,
@@ -159,7 +178,8 @@ def multi_member(seed: int = 1236, members: int = 2048, member_bytes: int = 2 <<
     plain = [np.concatenate(plains)] if keep_plain else []
     return Workload("multi_member", [comp], [members * member_bytes], plain,
                     {"members": members, "member_bytes": member_bytes,
-                     "types": types.tolist(), "levels": levels.tolist()})
+                     "types": types.tolist(), "levels": levels.tolist(),
+                     "member_comp_bytes": [int(x.size) for x in parts]})
 
 
 def lognormal_sizes(rng, n, median=64 << 10, sigma=1.5, lo=1 << 10, hi=64 << 20):

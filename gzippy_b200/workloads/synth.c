@@ -14,10 +14,13 @@
  * (deflateInit2(level, Z_DEFLATED, 31, 8, strategy)): levels 6 and 9 use
  * Z_DEFAULT_STRATEGY (dynamic blocks, stored for incompressible data) and
  * level 1 uses Z_FIXED, so level-1 members are fixed-Huffman as the
- * workload definition requires.  Large single members are compressed
- * pigz-style: blocks compressed in parallel, each primed with the previous
- * 32 KiB as its dictionary and closed with Z_SYNC_FLUSH, then framed as ONE
- * gzip member (one header, one CRC32/ISIZE trailer).
+ * workload definition requires.  Every member is one serial deflate stream
+ * (syn_gzip) unless a caller asks for the pigz-style framing
+ * (syn_gzip_parallel): blocks compressed in parallel, each primed with the
+ * previous 32 KiB as its dictionary and closed with Z_SYNC_FLUSH, then
+ * framed as ONE gzip member.  Each Z_SYNC_FLUSH leaves a byte-aligned empty
+ * stored block in the stream, a free block boundary a serial encoder would
+ * not write, so that framing is kept only as a separately named workload.
  */
 #include <math.h>
 #include <pthread.h>

@@ -103,11 +103,14 @@ def test_decode_chunks_match_oracle(G, ring):
         assert np.array_equal(ent[i, :r.out_len], e), i
 
 
+@pytest.mark.parametrize("encoder", ["zlib-serial", "pigz"])
 @pytest.mark.parametrize("ring", [False, True], ids=["pages", "ring"])
-def test_single_member_chunked_pipeline(G, ring):
+def test_single_member_chunked_pipeline(G, ring, encoder):
+    """One member of mixed content, as one serial deflate stream and in the
+    pigz-style framing (an empty stored block every MiB)."""
     parts = [W.content(t % 4, 100 + t, 1 << 20) for t in range(12)]
     plain = np.concatenate(parts)
-    c = W.gzip_member(plain, 6, threads=4)
+    c = W.encode_member(plain, 6, encoder, threads=4)
     for cb in (16 << 10, 64 << 10, 1 << 20):
         ctx = G.Context(chunk_bytes=cb, ring_history=ring)
         got = ctx.decompress(c)
