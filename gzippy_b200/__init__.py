@@ -517,7 +517,9 @@ def decompress_device_noalloc(d_in: int, in_len: int, d_out: int, out_cap: int,
         return 0
     if rc != OK:
         if rc == OUT_TOO_SMALL:
-            raise GzippyError("Decompression", f"output needs {n.value} bytes", rc)
+            e = GzippyError("Decompression", f"output needs {n.value} bytes", rc)
+            e.needed = n.value
+            raise e
         _raise(rc)
     return n.value
 

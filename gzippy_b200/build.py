@@ -22,8 +22,8 @@ def _stale() -> bool:
     if not os.path.exists(LIB):
         return True
     t = os.path.getmtime(LIB)
-    deps = sources() + glob.glob(os.path.join(CSRC, "*.cuh")) + [
-        os.path.join(ROOT, "include", "gzgpu.h")]
+    deps = (sources() + glob.glob(os.path.join(CSRC, "*.cuh")) +
+            glob.glob(os.path.join(CSRC, "*.h")) + glob.glob(os.path.join(ROOT, "include", "*.h")))
     return any(os.path.getmtime(d) > t for d in deps)
 
 

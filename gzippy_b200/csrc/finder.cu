@@ -23,11 +23,15 @@ constexpr uint64_t kFinderWindow = 1024;
 // Stored block starts, searched first for every speculative chunk: the first
 // one (by byte offset, hence by start bit) in [guess_bit, limit_bit) whose
 // successor passes stored_successor_ok becomes the chunk's start, and the
-// sync search and the block finder skip the chunk.  Such a start is real
-// (a false one needs two LEN/NLEN matches in a row, or a LEN/NLEN match and
-// a valid dynamic header), while the raw bytes of stored blocks (text, runs)
-// walk as fixed-Huffman codes and would give false sync starts.  One CTA of
-// kStoredThreads per chunk, scanning that many byte offsets a round.
+// sync search and the block finder skip the chunk.  The successor check is
+// a heuristic: a false start needs two LEN/NLEN matches in a row, or a
+// LEN/NLEN match and a valid dynamic header, which is rare but possible.
+// Correctness does not rest on it: a false start only decodes garbage that
+// no predecessor hands over to, and the host chain walk repairs past it.
+// The pass runs before the sync search because the raw bytes of stored
+// blocks (text, runs) walk as fixed-Huffman codes and would give false sync
+// starts.  One CTA of kStoredThreads per chunk, scanning that many byte
+// offsets a round.
 constexpr int kStoredThreads = 256;
 
 __global__ void __launch_bounds__(kStoredThreads)

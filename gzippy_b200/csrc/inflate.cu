@@ -1483,6 +1483,7 @@ __global__ void __launch_bounds__(32)
   __syncwarp();
   int32_t status = kOk;
   uint64_t total = 0, pos = 0;
+  bool too_small = false;  // some member did not fit out_cap
   if (n < 2 || in[0] != 0x1f || in[1] != 0x8b) status = kNotGzip;
   for (uint32_t member = 0; status == kOk; member++) {
     if (member > 0 && (n - pos < 18 || in[pos] != 0x1f || in[pos + 1] != 0x8b)) break;
@@ -1525,20 +1526,19 @@ __global__ void __launch_bounds__(32)
       status = kNoAllocTooLarge;
       break;
     }
-    if (total + r.out_len > out_cap) {
-      status = kOutTooSmall;
-      total += r.out_len;  // at least this many bytes are needed
-      break;
-    }
     // pages were taken in order, so entry q sits at pages[q] (no markers:
-    // a member starts with the zero window)
-    for (uint64_t q = lane; q < r.out_len; q += 32) out[total + q] = (uint8_t)S->pages[q];
+    // a member starts with the zero window).  Once a member does not fit
+    // out_cap, later members are still decoded and checked, without being
+    // written, so that *out_len reports the exact size needed.
+    if (!too_small && total + r.out_len > out_cap) too_small = true;
+    if (!too_small)
+      for (uint64_t q = lane; q < r.out_len; q += 32) out[total + q] = (uint8_t)S->pages[q];
     __syncwarp();
-    // CRC32: each lane one slice, combined in order by lane 0
+    // CRC32 of the member's entries: each lane one slice, combined in order by lane 0
     const uint64_t per = (r.out_len + 31) / 32;
     const uint64_t b0 = min((uint64_t)lane * per, r.out_len), b1 = min(b0 + per, r.out_len);
     uint32_t c = 0xFFFFFFFFu;
-    for (uint64_t q = b0; q < b1; q++) c = (c >> 8) ^ crc_tab[(c ^ out[total + q]) & 0xFF];
+    for (uint64_t q = b0; q < b1; q++) c = (c >> 8) ^ crc_tab[(c ^ (uint32_t)S->pages[q]) & 0xFF];
     c = ~c;
     uint32_t crc = 0;
     for (int l = 0; l < 32; l++) {
@@ -1556,6 +1556,7 @@ __global__ void __launch_bounds__(32)
     pos = trailer + 8;
     if (pos >= n) break;
   }
+  if (status == kOk && too_small) status = kOutTooSmall;
   if (lane == 0) {
     S->status = status;
     S->out_len = total;
@@ -1598,9 +1599,15 @@ extern "C" int gzgpu_decompress_device_noalloc(const void* d_in, size_t in_len, 
   }
   cudaStream_t st = reinterpret_cast<cudaStream_t>(cuda_stream);
   NoAllocScratch* S = reinterpret_cast<NoAllocScratch*>(scratch);
-  noalloc_kernel<<<1, 32, 0, st>>>(reinterpret_cast<const uint8_t*>(d_in), in_len,
-                                   reinterpret_cast<uint8_t*>(d_out), out_cap, S);
-  if (cudaGetLastError() != cudaSuccess) return GZGPU_DEVICE_ERROR;
+  // cudaLaunchKernel reports this launch's own failure; the thread's
+  // last-error state, which may hold an earlier error of the caller's, is
+  // neither read nor cleared
+  const uint8_t* k_in = reinterpret_cast<const uint8_t*>(d_in);
+  uint64_t k_n = in_len, k_cap = out_cap;
+  uint8_t* k_out = reinterpret_cast<uint8_t*>(d_out);
+  void* args[] = {(void*)&k_in, (void*)&k_n, (void*)&k_out, (void*)&k_cap, (void*)&S};
+  if (cudaLaunchKernel((const void*)noalloc_kernel, dim3(1), dim3(32), args, 0, st) != cudaSuccess)
+    return GZGPU_DEVICE_ERROR;
   struct {
     int32_t status;
     uint32_t pad;

@@ -193,7 +193,10 @@ int gzgpu_decompress_batch_device(gzgpu_ctx *ctx, const void *d_in, const uint64
  * (on different streams, or from different threads) race and must not be
  * issued; calls ordered on one stream are fine.  The call waits for its
  * stream to finish the decode and returns the status; *out_len = bytes
- * written (or needed, on GZGPU_OUT_TOO_SMALL). */
+ * written, or on GZGPU_OUT_TOO_SMALL the exact size of the whole stream
+ * (every member is still decoded and checked; members from the first one
+ * that does not fit are not written).  The launch's own failure returns
+ * GZGPU_DEVICE_ERROR; the thread's last-error state is left as it was. */
 #define GZGPU_NOALLOC_MAX_OUT (4u << 20)
 int gzgpu_decompress_device_noalloc(const void *d_in, size_t in_len, void *d_out, size_t out_cap,
                                     size_t *out_len, void *cuda_stream);

@@ -7,7 +7,11 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
-REFERENCE_BLOCKS = "/root/reference/corpus/silesia_blocks"
+# The reference project's checkout (JackDanger/gzippy), when one is mounted:
+# GZIPPY_REFERENCE names its root (default: a "reference" directory beside
+# this repository); tests that read its fixtures skip without it.
+REFERENCE_ROOT = os.environ.get("GZIPPY_REFERENCE", os.path.join(os.path.dirname(ROOT), "reference"))
+REFERENCE_BLOCKS = os.path.join(REFERENCE_ROOT, "corpus", "silesia_blocks")
 
 
 def pytest_configure(config):

@@ -479,3 +479,20 @@ def test_sync_start_naming_a_fixed_block_header(ctx):
     assert st == O.OK and int(res[0, 4]) == st
     assert int(res[0, 0]) == r.end_bit and int(res[0, 1]) == r.out_len
     assert np.array_equal(ent[0, :r.out_len], e)
+
+
+def test_planted_false_stored_start(G, ctx):
+    """A stored-block payload that holds a LEN/NLEN pair followed by a second
+    one passes the stored start rule: the finder takes it as its partition's
+    start (like the oracle) and the chain walk still returns the exact
+    plaintext."""
+    from test_oracle import planted_false_stored_start
+    comp, plain, len_off = planted_false_stored_start()
+    f = len_off * 8 - 2000
+    got = ctx.debug_find(comp, [(f, f + 8000)])
+    assert got[0] == _expected_start(comp, f, f + 8000)
+    assert got[0][1] == len_off * 8 - 3
+    for cb in (16 << 10, 32 << 10):
+        c2 = G.Context(chunk_bytes=cb)
+        assert c2.decompress(comp) == plain
+        c2.close()

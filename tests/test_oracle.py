@@ -205,3 +205,36 @@ def test_find_starts_keeps_true_stored_starts():
         false_ref = [x for x in ref if not any(x[0] <= t <= x[1] for t in true_set)]
         false_got = [x for x in got if not any(x[0] <= t <= x[1] for t in true_set)]
         assert len(false_got) <= len(false_ref) and len(false_got) <= 1, (level, len(false_ref), len(false_got))
+
+
+def planted_false_stored_start(seed: int = 11):
+    """A level-0 member (stored blocks only) of Markov text whose payload
+    holds a planted false stored start: a byte below 0x20 (three zero header
+    bits), LEN/NLEN, LEN bytes, then a second LEN/NLEN pair where the
+    successor would sit.  Returns (compressed, plaintext, planted byte offset
+    of the false LEN field in the compressed stream)."""
+    text = bytearray(W.content(W.MARKOV, seed, 300_000).tobytes())
+    plant = bytes([0x00, 0x10, 0x00, 0xEF, 0xFF]) + b"A" * 16 + bytes([0x00, 0x08, 0x00, 0xF7, 0xFF])
+    at = 150_003
+    text[at:at + len(plant)] = plant
+    comp = W.gzip_member(np.frombuffer(bytes(text), np.uint8), 0)
+    off = comp.tobytes().find(plant)
+    assert off > 0
+    return comp, bytes(text), off + 1
+
+
+def test_planted_false_stored_start_is_repaired():
+    """The stored start rule is a heuristic: a planted LEN/NLEN pair followed
+    by a second one passes it.  The partition holding the plant takes it as
+    its start, and the chain walk still returns the exact plaintext."""
+    comp, plain, len_off = planted_false_stored_start()
+    chunk = 4096
+    _, hl = O.gzip_header_len(comp)
+    b0 = hl * 8
+    part = (len_off * 8 - b0) // (chunk * 8)
+    lo, hi = b0 + part * chunk * 8, b0 + (part + 1) * chunk * 8
+    first, seek = O.find_starts(comp, lo, hi)
+    assert len(first) and int(seek[0]) == len_off * 8 - 3, "the plant is the partition's start"
+    st, out, stats = O.decompress_chunked(comp, chunk_bytes=chunk, threads=4)
+    assert st == O.OK and out.tobytes() == plain
+    assert stats.n_spec_rejected + stats.n_repairs >= 1

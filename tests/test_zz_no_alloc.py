@@ -6,10 +6,10 @@ synchronisation cudaMalloc/cudaFree may cause, or processes whose device
 memory is reserved up front by another framework.  For them the library decodes with a fixed
 device array instead of allocating.  This test calls that entry point
 through the C ABI and checks its output byte for byte against the regular
-entry point (gzgpu_decompress) -- integer work, so equality is exact -- on
-two calls in a row, since every call reuses the same array.  It lives in its
-own file, collected last, and passes in a fresh process as well as after the
-other tests."""
+entry point (gzgpu_decompress) and against the plaintext the stream was
+made from -- integer work, so equality is exact -- on two calls in a row,
+since every call reuses the same array.  It lives in its own file, collected
+last, and passes in a fresh process as well as after the other tests."""
 import zlib
 
 import numpy as np
@@ -29,14 +29,16 @@ def _cases():
     rnd = W.content(W.RANDOM, 22, 600_000).tobytes()
     runs = W.content(W.RUNS, 23, 2 << 20).tobytes()
     ramps = W.content(W.RAMPS, 24, 300_000).tobytes()
+    # name -> (gzip stream, the plaintext it decodes to)
     return {
-        "text_l6": _gz(text, 6),
-        "random_stored": _gz(rnd, 6),
-        "runs_l9": _gz(runs, 9),
-        "text_fixed_l1": _gz(text[:500_000], 1, zlib.Z_FIXED),
-        "multi_member": _gz(ramps, 6) + _gz(b"") + _gz(text[:100_000], 9),
-        "trailing_garbage": _gz(ramps[:50_000], 6) + b"\x00not a member",
-        "empty_member": _gz(b""),
+        "text_l6": (_gz(text, 6), text),
+        "random_stored": (_gz(rnd, 6), rnd),
+        "runs_l9": (_gz(runs, 9), runs),
+        "text_fixed_l1": (_gz(text[:500_000], 1, zlib.Z_FIXED), text[:500_000]),
+        "multi_member": (_gz(ramps, 6) + _gz(b"") + _gz(text[:100_000], 9),
+                         ramps + text[:100_000]),
+        "trailing_garbage": (_gz(ramps[:50_000], 6) + b"\x00not a member", ramps[:50_000]),
+        "empty_member": (_gz(b""), b""),
     }
 
 
@@ -53,8 +55,9 @@ def test_noalloc_matches_regular_entry_point_twice():
     import torch
     import gzippy_b200 as G
     ctx = G.Context()
-    for name, blob in _cases().items():
+    for name, (blob, plain) in _cases().items():
         ref = ctx.decompress(blob)
+        assert ref == plain, name
         d_in, d_out = _device(blob, len(ref) + 64)
         for call in range(2):
             d_out.fill_(0xA5)  # stale bytes cannot pass for output
@@ -62,8 +65,31 @@ def test_noalloc_matches_regular_entry_point_twice():
             n = G.decompress_device_noalloc(d_in.data_ptr(), len(blob), d_out.data_ptr(),
                                             d_out.numel())
             assert n == len(ref), (name, call)
-            assert d_out[:n].cpu().numpy().tobytes() == ref, (name, call)
+            got = d_out[:n].cpu().numpy().tobytes()
+            assert got == ref and got == plain, (name, call)
     ctx.close()
+
+
+def test_noalloc_out_too_small_reports_the_whole_stream():
+    """A multi-member stream whose second member does not fit: the call
+    reports the exact size of all members, and writes nothing past out_cap."""
+    import gzippy_b200 as G
+    from gzippy_b200 import workloads as W
+    parts = [W.content(t, 30 + t, 150_000 + 10_000 * t).tobytes() for t in range(4)]
+    blob = b"".join(_gz(p, 6) for p in parts)
+    total = sum(len(p) for p in parts)
+    d_in, d_out = _device(blob, total + 64)
+    for cap in (len(parts[0]) + 10, 1000, total - 1):
+        for _ in range(2):
+            d_out.fill_(0xA5)
+            with pytest.raises(G.GzippyError) as ei:
+                G.decompress_device_noalloc(d_in.data_ptr(), len(blob), d_out.data_ptr(), cap)
+            assert ei.value.code == G.OUT_TOO_SMALL
+            assert ei.value.needed == total, cap
+            assert bool(d_out[cap:].eq(0xA5).all())
+    # with the size it reported, the same call succeeds
+    n = G.decompress_device_noalloc(d_in.data_ptr(), len(blob), d_out.data_ptr(), total)
+    assert n == total and d_out[:n].cpu().numpy().tobytes() == b"".join(parts)
 
 
 def _code(fn):
