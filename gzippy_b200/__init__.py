@@ -52,7 +52,8 @@ class Config(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("chunk_bytes", ctypes.c_size_t),
                 ("lut_bits", ctypes.c_int), ("autotune", ctypes.c_int),
                 ("ring_history", ctypes.c_int), ("ctas_per_sm", ctypes.c_int),
-                ("fine_split", ctypes.c_int), ("high_priority", ctypes.c_int)]
+                ("fine_split", ctypes.c_int), ("high_priority", ctypes.c_int),
+                ("work_order", ctypes.c_int)]
 
 
 class Span(ctypes.Structure):
@@ -72,7 +73,8 @@ class Stats(ctypes.Structure):
                   "n_rejected", "n_repairs", "n_tail_marker_chunks", "n_pages", "decode_passes",
                   "kernel_launches", "chunk_bytes")] +
                 [("lut_bits", ctypes.c_int32), ("ctas_per_sm", ctypes.c_int32),
-                 ("tune_key", ctypes.c_uint32), ("tune_trials", ctypes.c_uint32)])
+                 ("tune_key", ctypes.c_uint32), ("tune_trials", ctypes.c_uint32),
+                 ("pool_regrows", ctypes.c_uint32), ("reserved", ctypes.c_uint32)])
 
     def as_dict(self) -> dict:
         return {n: getattr(self, n) for n, _ in self._fields_}
@@ -171,10 +173,11 @@ class Context:
 
     def __init__(self, device: int = 0, chunk_bytes: int = 0, lut_bits: int = 0,
                  autotune: bool = False, ring_history: bool = False, ctas_per_sm: int = 0,
-                 fine_split: bool = False, high_priority: bool = False):
+                 fine_split: bool = False, high_priority: bool = False,
+                 longest_first: bool = True):
         self._lib = lib()
         cfg = Config(device, chunk_bytes, lut_bits, int(autotune), int(ring_history), ctas_per_sm,
-                     int(fine_split), int(high_priority))
+                     int(fine_split), int(high_priority), 0 if longest_first else 1)
         h = ctypes.c_void_p()
         rc = self._lib.gzgpu_create(ctypes.byref(h), ctypes.byref(cfg))
         if rc != OK:

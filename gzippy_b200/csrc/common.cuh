@@ -50,6 +50,11 @@ enum : uint32_t {
                            // non-final fixed-Huffman block)
   kChunkPiece = 16u,       // a piece of a partition cut by its output estimate
 };
+// flags bits 24..31: the chunk's first decode attempt number (its pages carry
+// attempt numbers from there; raised when a chunk is decoded again after the
+// page pool ran out, so its old pages never pass for the new ones)
+constexpr int kGenBaseShift = 24;
+constexpr uint32_t kGenBaseMax = 255;
 
 // Sync starts in fixed-Huffman data: positions are walked from kSyncOffsets
 // consecutive start bits to the first symbol boundary at or past

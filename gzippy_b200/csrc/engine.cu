@@ -53,6 +53,19 @@ struct DevBuf {
     if (e == cudaSuccess) cap = want;
     return e;
   }
+  // grow to at least n bytes, keeping the first `keep` bytes
+  cudaError_t grow_keep(size_t n, size_t keep) {
+    if (n <= cap) return cudaSuccess;
+    void* q = nullptr;
+    const size_t want = n + n / 4 + 4096;
+    cudaError_t e = cudaMallocAsync(&q, want, st);
+    if (e != cudaSuccess) return e;
+    if (p && keep) e = cudaMemcpyAsync(q, p, std::min(keep, cap), cudaMemcpyDeviceToDevice, st);
+    if (p) cudaFreeAsync(p, st);
+    p = q;
+    cap = want;
+    return e;
+  }
   void release() {
     if (p) cudaFreeAsync(p, st);
     p = nullptr;
@@ -168,6 +181,7 @@ struct gzgpu_ctx {
   int ctas_per_sm = 3;  // page kernel CTAs per SM (3 or 4)
   bool fine_split = false;  // output-estimate pieces + dynamic-block sync starts
   bool high_priority = false;  // stream at the device's greatest priority
+  bool lpt = true;             // decode work list longest-first (else in stream order)
   bool job_raw = false;        // the job's streams are raw DEFLATE (no gzip framing)
   bool job_sync = true;     // the running job has sync starts (decoder variant)
   int decode_blocks = 0;
@@ -176,7 +190,7 @@ struct gzgpu_ctx {
   gzgpu_stats stats{};
   bool crc_ready = false;
 
-  DevBuf in, out, s_off, s_len, info, units, cands, counters, descs, results, spec, work;
+  DevBuf in, out, s_off, s_len, info, units, cands, counters, descs, results, spec, work, cost;
   DevBuf pages, owner, seq, placed, placed_of, list, segs, cblocks, bcrcs, mblk, mtrail, mlen,
       mcrc, mstatus;
   // seek-index builds: the decoder's block log, the checkpoint interval and
@@ -191,7 +205,8 @@ struct gzgpu_ctx {
   std::vector<DevBuf*> all_bufs() {
     return {&in,     &out,   &s_off,   &s_len,  &info,   &units,   &cands,  &counters, &descs,
             &results, &spec, &work,    &pages,  &owner,  &seq,     &placed, &placed_of, &list,
-            &segs,   &cblocks, &bcrcs, &mblk,   &mtrail, &mlen,    &mcrc,   &mstatus, &blk_log};
+            &segs,   &cblocks, &bcrcs, &mblk,   &mtrail, &mlen,    &mcrc,   &mstatus, &blk_log,
+            &cost};
   }
   const uint8_t* cur_in = nullptr;  // input buffer of the running job
   uint8_t* user_out = nullptr;       // caller device output (device-resident API)
@@ -248,8 +263,16 @@ struct gzgpu_ctx {
   }
 
   int run(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R);
+  uint32_t pool_cap() const {
+    return (uint32_t)std::min<uint64_t>(pages.cap / (kPageEntries * 2),
+                                        std::min(owner.cap, seq.cap) / 4);
+  }
+  // decode again, in a grown page pool, the chunks of [b, e) that ran out of pages
+  int regrow(std::vector<ChunkDesc>& hd, std::vector<ChunkResult>& hr, uint32_t b, uint32_t e,
+             float& ms_kernel);
   // run() under the autotuner when it is on
   int job(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R);
+  int job_tuned(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R);
 
   // Autotuner: per kind of job (key), the fastest decode parameters found.
   struct TuneCfg {
@@ -286,7 +309,25 @@ static uint64_t pick_chunk_bytes(uint64_t in_len) {
   return c;
 }
 
+// Internal statuses that reach a caller as public codes: a page pool that
+// could not grow (device memory) and a chunk left undecoded are device
+// errors; a decode that ran past its stop is invalid deflate data.
+static int public_status(int st) {
+  switch (st) {
+    case kPoolExhausted:
+    case kNotDecoded: return GZGPU_DEVICE_ERROR;
+    case kOvershoot: return GZGPU_BAD_DEFLATE;
+    default: return st;
+  }
+}
+
 int gzgpu_ctx::job(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R) {
+  const int rc = job_tuned(S, R);
+  for (StreamOut& r : R) r.status = public_status(r.status);
+  return public_status(rc);
+}
+
+int gzgpu_ctx::job_tuned(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R) {
   if (!autotune) return run(S, R);
   uint64_t total_in = 0;
   for (const StreamSpec& s : S) total_in += s.len;
@@ -337,6 +378,66 @@ int gzgpu_ctx::job(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R) 
   rc = run(S, R);
   stats.tune_trials = trials;
   return rc;
+}
+
+int gzgpu_ctx::regrow(std::vector<ChunkDesc>& hd, std::vector<ChunkResult>& hr, uint32_t b,
+                      uint32_t e, float& ms_kernel) {
+  int rc;
+  for (;;) {
+    std::vector<uint32_t> ids;
+    uint64_t extra = 0;  // pages the failed chunks are expected to need
+    for (uint32_t i = b; i < e; i++) {
+      if (!(hd[i].flags & kChunkValid) || hr[i].status != kPoolExhausted) continue;
+      ids.push_back(i);
+      const ChunkDesc& d = hd[i];
+      const ChunkResult& r = hr[i];
+      // output so far, extrapolated over the chunk's compressed range, and
+      // never above deflate's ceiling of 1032 output bytes per input byte
+      const uint64_t end = std::min<uint64_t>(d.stop_lo, d.in_end * 8);
+      const uint64_t span = end > d.start_bit ? end - d.start_bit : 8;
+      const uint64_t done = r.end_bit > d.start_bit ? r.end_bit - d.start_bit : 1;
+      const double want = (double)r.out_len * (double)span / (double)done * 1.25;
+      const double ceil = 1032.0 * (double)span / 8.0 + 258.0;
+      extra += (uint64_t)(std::min(want, ceil) / kPageEntries) + 3;
+      if ((d.flags >> kGenBaseShift) + 2 * kMaxTries > kGenBaseMax) return kPoolExhausted;
+    }
+    if (ids.empty()) return kOk;
+    uint32_t used = 0;
+    if ((rc = check(cudaMemcpyAsync(&used, counters.as<uint32_t>() + 2, 4, cudaMemcpyDeviceToHost,
+                                    st))) ||
+        (rc = check(cudaStreamSynchronize(st))))
+      return rc;
+    const uint64_t cap0 = pool_cap();
+    used = (uint32_t)std::min<uint64_t>(used, cap0);
+    const uint64_t need = std::max<uint64_t>(used + extra + 64, cap0 + cap0 / 4);
+    if (need >= kNoPage) return kPoolExhausted;
+    if ((rc = check(pages.grow_keep(need * kPageEntries * 2, (uint64_t)used * kPageEntries * 2))) ||
+        (rc = check(owner.grow_keep(4 * need, 4ull * used))) ||
+        (rc = check(seq.grow_keep(4 * need, 4ull * used))))
+      return rc;
+    stats.pool_regrows++;
+    // the failed chunks start over with attempt numbers past their old pages'
+    for (uint32_t i : ids) {
+      const uint32_t g = std::min<uint32_t>(hr[i].gen + 1, kGenBaseMax);
+      hd[i].flags = (hd[i].flags & ((1u << kGenBaseShift) - 1)) | (g << kGenBaseShift);
+      cudaMemcpyAsync(descs.as<ChunkDesc>() + i, &hd[i], sizeof(ChunkDesc), cudaMemcpyHostToDevice, st);
+    }
+    const uint32_t nw = (uint32_t)ids.size();
+    cudaMemcpyAsync(work.p, ids.data(), 4ull * nw, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(counters.as<uint32_t>() + 1, &nw, 4, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(counters.as<uint32_t>() + 2, &used, 4, cudaMemcpyHostToDevice, st);
+    cudaEventRecord(ev[8], st);
+    if ((rc = check(launch_decode(counters.as<uint32_t>() + 1)))) return rc;
+    cudaEventRecord(ev[9], st);
+    cudaMemcpyAsync(hd.data() + b, descs.as<ChunkDesc>() + b, sizeof(ChunkDesc) * (e - b),
+                    cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(hr.data() + b, results.as<ChunkResult>() + b, sizeof(ChunkResult) * (e - b),
+                    cudaMemcpyDeviceToHost, st);
+    if ((rc = check(cudaStreamSynchronize(st)))) return rc;
+    float t = 0;
+    cudaEventElapsedTime(&t, ev[8], ev[9]);
+    ms_kernel += t;
+  }
 }
 
 int gzgpu_ctx::run(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R) {
@@ -616,11 +717,12 @@ int gzgpu_ctx::run(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R) 
     }
   }
   stats.n_chunks = n_grid;
-  if ((rc = check(launch_link(descs.as<ChunkDesc>(), n_grid, work.as<uint32_t>(),
-                              counters.as<uint32_t>() + 1, std::max<uint64_t>(cbits, 1ull << 21),
-                              st))))
+  if (lpt && (rc = check(cost.ensure(4 * (size_t)(n_grid + 1))))) return rc;
+  if ((rc = check(launch_link(cur_in, descs.as<ChunkDesc>(), n_grid, work.as<uint32_t>(),
+                              counters.as<uint32_t>() + 1, lpt ? cost.as<float>() : nullptr,
+                              std::max<uint64_t>(cbits, 1ull << 21), st))))
     return rc;
-  stats.kernel_launches += 1;
+  stats.kernel_launches += lpt ? 2 : 1;
   {
     // the decoder variant without sync-start handling when there are none
     uint32_t h_sync = 1;
@@ -631,16 +733,19 @@ int gzgpu_ctx::run(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R) 
   }
   cudaEventRecord(ev[4], st);
   // ---- 4. decode ----------------------------------------------------------
+  // The pool is sized from the members' ISIZEs (raw streams: 4 x their
+  // input).  ISIZE is only a hint (it wraps past 4 GiB, and a raw stream has
+  // none): the chunks that run out of pages are decoded again in a grown
+  // pool, the others keep theirs (regrow).
   uint64_t pages_needed = (est_out + n_grid * (uint64_t)kPageEntries) / kPageEntries + 64;
   std::vector<ChunkResult> hr;
   float ms_dec_kernel = 0;
-  for (int attempt = 0;; attempt++) {
+  {
     if ((rc = check(pages.ensure(pages_needed * kPageEntries * 2))) ||
         (rc = check(owner.ensure(4 * pages_needed))) || (rc = check(seq.ensure(4 * pages_needed))))
       return rc;
     cudaMemsetAsync(counters.as<uint32_t>() + 2, 0, 4, st);
     if (job_index) {
-      // the block log restarts with every full decode pass
       blk_cap = (uint32_t)std::min<uint64_t>(std::max<uint64_t>(blk_need, total_in / 64 + 65536),
                                              1u << 30);
       if ((rc = check(blk_log.ensure(sizeof(BlockRec) * (uint64_t)blk_cap)))) return rc;
@@ -659,12 +764,7 @@ int gzgpu_ctx::run(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R) 
     float t = 0;
     cudaEventElapsedTime(&t, ev[8], ev[9]);
     ms_dec_kernel += t;
-    bool exhausted = false;
-    for (uint32_t i = 0; i < n_grid; i++)
-      if ((hd[i].flags & kChunkValid) && hr[i].status == kPoolExhausted) exhausted = true;
-    if (!exhausted) break;
-    if (attempt >= 6) return kPoolExhausted;
-    pages_needed *= 2;
+    if ((rc = regrow(hd, hr, 0, n_grid, ms_dec_kernel))) return rc;
   }
   cudaEventRecord(ev[5], st);
   // ---- 5. chain walk with repairs (host) ---------------------------------
@@ -929,8 +1029,7 @@ int gzgpu_ctx::run(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R) 
     float t = 0;
     cudaEventElapsedTime(&t, ev[8], ev[9]);
     ms_dec_kernel += t;
-    for (uint32_t k = 0; k < nr; k++)
-      if (hr[base_id + k].status == kPoolExhausted) return kPoolExhausted;
+    if ((rc = regrow(hd, hr, base_id, base_id + nr, ms_dec_kernel))) return rc;
     for (auto& sw : SW) {
       for (Walker& w : sw) {
         if (w.pending >= 0) {
@@ -1028,9 +1127,8 @@ int gzgpu_ctx::run(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R) 
   uint32_t n_pages_used = 0;
   cudaMemcpyAsync(&n_pages_used, counters.as<uint32_t>() + 2, 4, cudaMemcpyDeviceToHost, st);
   if ((rc = check(cudaStreamSynchronize(st)))) return rc;
-  const uint32_t pool_cap = (uint32_t)std::min<uint64_t>(pages.cap / (kPageEntries * 2),
-                                                         std::min(owner.cap, seq.cap) / 4);
-  n_pages_used = std::min(n_pages_used, pool_cap);
+  const uint32_t pcap = pool_cap();
+  n_pages_used = std::min(n_pages_used, pcap);
   stats.n_pages = n_pages_used;
   cur_out = (user_out && out_total <= user_cap) ? user_out : nullptr;
   if ((rc = check(cur_out ? cudaSuccess : out.ensure(out_total + 64))) ||
@@ -1058,7 +1156,7 @@ int gzgpu_ctx::run(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R) 
   }
   if (!cur_out) cur_out = out.as<uint8_t>();
   PagePool pool{pages.as<uint16_t>(), owner.as<uint32_t>(), seq.as<uint32_t>(),
-                counters.as<uint32_t>() + 2, pool_cap};
+                counters.as<uint32_t>() + 2, pcap};
   cudaEventRecord(ev[10], st);
   if (!crc_ready) {
     if ((rc = check(resolve_init(st)))) return rc;
@@ -1228,6 +1326,7 @@ int gzgpu_create(gzgpu_ctx** out, const gzgpu_config* cfg) {
     if (cfg->ctas_per_sm == 3 || cfg->ctas_per_sm == 4) c->ctas_per_sm = cfg->ctas_per_sm;
     c->fine_split = cfg->fine_split != 0;
     c->high_priority = cfg->high_priority != 0;
+    c->lpt = cfg->work_order == 0;
   }
   if (cudaSetDevice(c->dev) != cudaSuccess) {
     delete c;

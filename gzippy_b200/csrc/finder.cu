@@ -177,8 +177,32 @@ __global__ void __launch_bounds__(kSyncOffsets)
 // A speculative start may be a phantom whose garbage code table never fails;
 // such a chunk gives up `slack` bits past its stop and the chain walk
 // re-decodes the gap from the confirmed boundary instead.
-__global__ void link_kernel(ChunkDesc* descs, uint32_t n, uint32_t* work, uint32_t* n_work,
-                            uint64_t slack) {
+// Decode cost of a linked chunk, in output-byte equivalents: its expected
+// output (the output-per-input estimate of the dynamic header it starts in,
+// times the compressed bits up to its stop), with stored starts counted at
+// a tenth since stored blocks decode as bulk copies.
+__device__ float chunk_cost(const uint8_t* __restrict__ in, const ChunkDesc& d, uint64_t stop) {
+  const uint64_t nbits = d.in_end * 8;
+  uint64_t end = stop != kNoStop ? stop : nbits;
+  if (end > nbits) end = nbits;
+  const float span = end > d.start_bit ? (float)(end - d.start_bit) * 0.125f : 0.f;
+  float r = d.est_ratio;
+  if (!(r > 0.f)) {
+    // member starts and sync starts carry no finder estimate: take it from
+    // the header of the block they start in
+    const uint64_t hdr = (d.flags & kChunkSync) ? d.table_bit : d.start_bit;
+    const uint32_t bt = hdr ? (uint32_t)(peek_bits(in, d.in_end, hdr, 3) >> 1) : 1u;
+    if (bt == 2) r = dyn_header_ratio(in, d.in_end, hdr);
+    else if (bt == 0) r = 0.1f;
+    if (!(r > 0.f)) r = 2.f;  // fixed-Huffman data: about 2 bytes per input byte
+  } else if (r == 1.f && (peek_bits(in, d.in_end, d.start_bit, 3) >> 1) == 0) {
+    r = 0.1f;  // a stored start
+  }
+  return r * span;
+}
+
+__global__ void link_kernel(const uint8_t* __restrict__ in, ChunkDesc* descs, uint32_t n,
+                            uint32_t* work, uint32_t* n_work, float* cost, uint64_t slack) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   ChunkDesc& d = descs[i];
@@ -211,7 +235,40 @@ __global__ void link_kernel(ChunkDesc* descs, uint32_t n, uint32_t* work, uint32
   if ((d.flags & kChunkSync) && stop != kNoStop && stop > d.start_bit)
     s = min(slack, max(stop - d.start_bit, (uint64_t)kSyncMinSlack));
   d.abort_bit = (stop != kNoStop && !(d.flags & kChunkMemberFirst)) ? stop + s : kNoStop;
-  work[atomicAdd(n_work, 1u)] = i;
+  if (cost) cost[i] = chunk_cost(in, d, stop);
+  else work[atomicAdd(n_work, 1u)] = i;
+}
+
+// The decode work list in descending cost (longest processing time first),
+// so that the persistent decoder starts the longest chunks first and the
+// short ones fill in at the end.  One CTA: a histogram over half-octave cost
+// buckets, a scan, and a scatter (order inside a bucket is arbitrary).
+constexpr int kCostBuckets = 64;
+__global__ void __launch_bounds__(1024)
+    order_kernel(const ChunkDesc* __restrict__ descs, const float* __restrict__ cost, uint32_t n,
+                 uint32_t* work, uint32_t* n_work) {
+  __shared__ uint32_t hist[kCostBuckets], base[kCostBuckets];
+  if (threadIdx.x < kCostBuckets) hist[threadIdx.x] = 0;
+  __syncthreads();
+  auto bucket = [&](uint32_t i) {
+    const float c = fmaxf(cost[i], 0.f) + 1.f;
+    const int b = (int)(2.f * __log2f(c));
+    return kCostBuckets - 1 - min(max(b, 0), kCostBuckets - 1);  // costliest first
+  };
+  for (uint32_t i = threadIdx.x; i < n; i += blockDim.x)
+    if (descs[i].flags & kChunkValid) atomicAdd(&hist[bucket(i)], 1u);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t a = 0;
+    for (int b = 0; b < kCostBuckets; b++) {
+      base[b] = a;
+      a += hist[b];
+    }
+    *n_work = a;
+  }
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < n; i += blockDim.x)
+    if (descs[i].flags & kChunkValid) work[atomicAdd(&base[bucket(i)], 1u)] = i;
 }
 
 cudaError_t launch_finder(const uint8_t* in, ChunkDesc* descs, const uint32_t* spec,
@@ -227,10 +284,11 @@ cudaError_t launch_finder(const uint8_t* in, ChunkDesc* descs, const uint32_t* s
   return cudaGetLastError();
 }
 
-cudaError_t launch_link(ChunkDesc* descs, uint32_t n, uint32_t* work, uint32_t* n_work,
-                        uint64_t slack_bits, cudaStream_t stream) {
+cudaError_t launch_link(const uint8_t* in, ChunkDesc* descs, uint32_t n, uint32_t* work,
+                        uint32_t* n_work, float* cost, uint64_t slack_bits, cudaStream_t stream) {
   if (n == 0) return cudaSuccess;
-  link_kernel<<<(n + 255) / 256, 256, 0, stream>>>(descs, n, work, n_work, slack_bits);
+  link_kernel<<<(n + 255) / 256, 256, 0, stream>>>(in, descs, n, work, n_work, cost, slack_bits);
+  if (cost) order_kernel<<<1, 1024, 0, stream>>>(descs, cost, n, work, n_work);
   return cudaGetLastError();
 }
 

@@ -1176,10 +1176,13 @@ __device__ __forceinline__ void work_loop(const uint8_t* __restrict__ in, ChunkD
     if (lane == 0) asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
     const bool speculative =
         !(d.flags & (kChunkMemberFirst | kChunkSync)) && d.limit_bit > d.lo_bit;
-    for (uint32_t gen = 0;; gen++) {
+    // attempts are numbered from the chunk's generation base (a chunk decoded
+    // again after the page pool ran out tags its pages past the old ones)
+    const uint32_t gen0 = d.flags >> kGenBaseShift;
+    for (uint32_t gen = gen0;; gen++) {
       int32_t st = decode_chunk<LB, kRing, kSync>(in, d, descs, &results[cid], cid, gen, ring, T, pool,
                                            lane);
-      if (st == kOk || st == kPoolExhausted || !speculative || gen + 1 >= kMaxTries) break;
+      if (st == kOk || st == kPoolExhausted || !speculative || gen + 1 >= gen0 + kMaxTries) break;
       uint64_t lo = 0, hi = 0;
       if (!warp_find_first(in, d.in_end, d.lo_bit + 1, d.limit_bit, d.limit_bit, lane, lo, hi)) break;
       d.lo_bit = lo;

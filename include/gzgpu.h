@@ -70,6 +70,8 @@ typedef struct {
   int high_priority;  /* 1 = the context's stream has the device's greatest priority:
                          its pending thread blocks are scheduled before those of other
                          contexts' streams (running blocks are not preempted) */
+  int work_order;     /* order in which the persistent decoder takes chunks: 0 = longest
+                         expected decode first (default), 1 = in stream order */
 } gzgpu_config;
 
 typedef struct {
@@ -95,6 +97,9 @@ typedef struct {
   int32_t ctas_per_sm;
   uint32_t tune_key;    /* autotuner key of the last job (0 when autotune is off) */
   uint32_t tune_trials; /* decodes the autotuner ran for the last call (0 = cached) */
+  uint32_t pool_regrows; /* times the page pool was grown and the chunks that had run
+                            out of pages were decoded again */
+  uint32_t reserved;
 } gzgpu_stats;
 
 /* Create / destroy a context on cfg->device (NULL cfg = defaults). */

@@ -127,3 +127,64 @@ def test_device_stored_members():
             assert cx.decompress(comp) == plain == zlib.decompress(comp, 31), name
     finally:
         cx.close()
+
+
+def _zeros_deflate(n: int, wbits: int) -> bytes:
+    c = zlib.compressobj(6, zlib.DEFLATED, wbits)
+    z = bytes(16 << 20)
+    return b"".join(c.compress(z) for _ in range(n // len(z))) + c.flush()
+
+
+@pytest.mark.gpu
+def test_device_raw_and_zlib_high_ratio_grow_the_page_pool():
+    """256 MiB of zeros (about 1000:1) as raw DEFLATE and as zlib.  These
+    formats carry no ISIZE, so the page pool starts at 4x the input, far too
+    small: the chunks that run out of pages are decoded again in a grown pool
+    (up to deflate's 1032:1 ceiling), and the output is exact."""
+    import gzippy_b200 as G
+    n = 256 << 20
+    cx = G.Context()
+    try:
+        for wbits, fn in ((-15, cx.inflate_raw), (15, cx.inflate_zlib)):
+            comp = _zeros_deflate(n, wbits)
+            assert len(comp) * 500 < n
+            got = fn(comp)
+            assert len(got) == n and got.count(0) == n, wbits
+            assert cx.stats().pool_regrows >= 1
+    finally:
+        cx.close()
+
+
+@pytest.mark.gpu
+def test_device_member_over_4gib_with_wrapped_isize():
+    """A gzip member of 4 GiB + 1 MiB: its ISIZE trailer holds the size mod
+    2^32 (1 MiB), which sizes the page pool far too small.  The decode grows
+    the pool, the trailer check compares sizes mod 2^32 as RFC 1952 defines
+    ISIZE, and every byte lands in place (a period-1024 pattern, checked on
+    the device)."""
+    import torch
+    import gzippy_b200 as G
+    n = (4 << 30) + (1 << 20)
+    rng = np.random.default_rng(5)
+    blk = rng.integers(0, 256, 1024, dtype=np.uint8)
+    piece = np.tile(blk, 65536).tobytes()            # 64 MiB, a whole number of periods
+    c = zlib.compressobj(1, zlib.DEFLATED, 31)
+    parts = [c.compress(piece) for _ in range(n // len(piece))]
+    parts.append(c.compress(piece[: n % len(piece)]))
+    parts.append(c.flush())
+    comp = np.frombuffer(b"".join(parts), np.uint8)
+    assert int.from_bytes(comp[-4:].tobytes(), "little") == n % (1 << 32)
+    cx = G.Context()
+    try:
+        d_in = torch.zeros(comp.size + 1024, dtype=torch.uint8, device="cuda")
+        d_in[: comp.size] = torch.from_numpy(comp).cuda()
+        d_out = torch.empty(n + 4096, dtype=torch.uint8, device="cuda")
+        got = cx.decompress_device(d_in.data_ptr(), comp.size, d_out.data_ptr(), d_out.numel())
+        assert got == n
+        assert cx.stats().pool_regrows >= 1
+        want = torch.from_numpy(blk).cuda().repeat(n // 1024 + 1)[:n]
+        assert torch.equal(d_out[:n], want)
+        del want, d_out, d_in
+        torch.cuda.empty_cache()
+    finally:
+        cx.close()
