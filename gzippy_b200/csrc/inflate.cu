@@ -86,6 +86,7 @@ struct alignas(16) Tables {
   uint16_t pre_count[16], pre_first[16], pre_offs[16];
   uint16_t next[16];
   uint8_t lens[320];
+  uint8_t smap[32];  // output pass: lane of the symbol starting at each entry
 };
 
 template <int LB>
@@ -618,117 +619,119 @@ __device__ int32_t huff_block_parallel(BitReader& br, const Tables<LB>* T, PageH
       }
       info = total | (kind << 6) | (slow << 8) | (val << 16);
     }
-    // successor of a symbol starting here; 128 + lane stops the walk at a
-    // symbol that needs the full tables, ends the block or is invalid
-    // (chain positions stay below 32 + 48)
+    // The chain: each lane packs the successor of a symbol starting at its
+    // bit ([7:0]; 128 + lane when the symbol needs the full tables, ends the
+    // block or is invalid) with the entries it writes ([16:8]).  Walking the
+    // chain from bit 0 gives every symbol on it its output offset `excl`.
     const uint32_t kind0 = (info >> 6) & 3;
-    uint32_t nxt = ((info & 0x100) || kind0 >= kKindEob) ? 128u + lane : lane + (info & 63);
-    if (kSync && nxt == rt) nxt = 96;  // the walk ends at the sync start
-    // walk the chain of symbols that start in bits [0, 32)
-    uint32_t path = 0, p = 0;
-    bool eob = false;
-#pragma unroll
-    for (int k = 0; k < 8; k++) {
-      if (p < 32) {
-        path |= 1u << p;
-        p = __shfl_sync(0xFFFFFFFFu, nxt, p & 31);
+    const uint32_t pk = ((info & 0x100) || kind0 >= kKindEob)
+                            ? 128u + lane
+                            : (lane + (info & 63)) | ((kind0 == kKindLit ? 1u : (info >> 16)) << 8);
+    uint32_t p = 0, acc = 0, excl = 0;
+    bool on = false, eob = false, at_sync = false;
+    for (;;) {
+      const uint32_t v = __shfl_sync(0xFFFFFFFFu, pk, (int)p);
+      if (lane == (int)p) {
+        on = true;
+        excl = acc;
       }
-    }
-    while (p < 32 || p >= 128) {
-      if (p >= 128) {
-        const uint32_t sl = p - 128;  // on the path already
-        uint32_t ip = __shfl_sync(0xFFFFFFFFu, info, (int)sl);
-        if (ip & 0x100) {
-          uint32_t dd = 0;
-          // bits [sl, sl + 64) of the step
-          const uint32_t ts = (uint32_t)(pos & 31) + sl;
-          const uint32_t was = ts >> 5, bs = ts & 31;
-          const uint64_t l64 = was ? ((uint64_t)W[2] << 32 | W[1]) : ((uint64_t)W[1] << 32 | W[0]);
-          const uint32_t h32 = was ? W[3] : W[2];
-          ip = decode_symbol_full<LB>(bs ? (l64 >> bs) | ((uint64_t)h32 << (64 - bs)) : l64, T, &dd);
-          if (lane == (int)sl) {
-            info = ip;
-            dinfo = dd;
-          }
+      if ((v & 0xFF) >= 128) {
+        // the symbol at p with the full tables (the same in every lane)
+        uint32_t dd = 0;
+        const uint32_t ts = (uint32_t)(pos & 31) + p;
+        const uint32_t was = ts >> 5, bs = ts & 31;
+        const uint64_t l64 = was ? ((uint64_t)W[2] << 32 | W[1]) : ((uint64_t)W[1] << 32 | W[0]);
+        const uint32_t h32 = was ? W[3] : W[2];
+        const uint32_t ip =
+            decode_symbol_full<LB>(bs ? (l64 >> bs) | ((uint64_t)h32 << (64 - bs)) : l64, T, &dd);
+        if (lane == (int)p) {
+          info = ip;
+          dinfo = dd;
         }
         const uint32_t kd = (ip >> 6) & 3;
         if (kd == kKindBad) {
           status = kBadDeflate;
           break;
         }
-        p = sl + (ip & 63);
+        p += ip & 63;
         if (kd == kKindEob) {
           eob = true;
           break;
         }
-        if (kSync && p == rt) p = 96;
-        continue;
+        acc += kd == kKindLit ? 1u : (ip >> 16);
+      } else {
+        acc += v >> 8;
+        p = v & 0xFF;
       }
-      path |= 1u << p;
-      p = __shfl_sync(0xFFFFFFFFu, nxt, p & 31);
-    }
-    if (status != kOk) break;
-    const bool at_sync = kSync && p == 96;
-    if (at_sync) p = rt;
-    // output offsets: exclusive prefix sum of output lengths along the chain
-    const bool on = (path >> lane) & 1;
-    const uint32_t kind = (info >> 6) & 3;
-    const uint32_t olen = on ? (kind == kKindLit ? 1u : (kind == kKindLen ? (info >> 16) : 0u)) : 0u;
-    uint32_t incl = olen;
-#pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-      uint32_t tt = __shfl_up_sync(0xFFFFFFFFu, incl, d);
-      if (lane >= d) incl += tt;
-    }
-    const uint32_t excl = incl - olen;
-    const uint32_t step_out = __shfl_sync(0xFFFFFFFFu, incl, 31);
-    const int32_t orel = (int32_t)(o - (ph.s << 16));  // o within page seq s
-    if (on && kind == kKindLit) *page_addr(ph, orel + (int32_t)excl) = (uint16_t)(info >> 16);
-    uint32_t mm = __ballot_sync(0xFFFFFFFFu, on && kind == kKindLen);
-    while (mm) {
-      __syncwarp();
-      const int src = __ffs(mm) - 1;
-      mm &= mm - 1;
-      const uint32_t len = __shfl_sync(0xFFFFFFFFu, info >> 16, src);
-      const uint32_t dist = __shfl_sync(0xFFFFFFFFu, dinfo, src);
-      const uint32_t mo = __shfl_sync(0xFFFFFFFFu, excl, src);
-      if ((uint64_t)dist > o + mo + kWindow) {
-        status = kBadDeflate;
+      if (kSync && p == rt) {  // the walk ends at the successor's sync start
+        at_sync = true;
         break;
       }
-      // entry po+j = entry po-dist+(j mod dist); every source is older than po
-      const int32_t prel = orel + (int32_t)mo;  // copy start, page-relative
-      const bool wrap = dist < len;
-      const uint32_t step_mod = wrap ? 32 % dist : 0;
-      uint32_t r = wrap ? (uint32_t)lane % dist : (uint32_t)lane;
-      // a source before the chunk's first entry is a window marker (or zero)
-      const int64_t before = (int64_t)(o + mo) - (int64_t)dist;  // chunk position of source j=0
-      for (uint32_t j0 = 0; j0 < len; j0 += 32) {
-        const uint32_t j = j0 + lane;
-        const bool act = j < len;
-        uint16_t v = 0;
-        if (act) {
-          const uint32_t sj = wrap ? r : j;
-          if (before + (int64_t)sj >= 0) {
-            v = *page_addr(ph, prel - (int32_t)dist + (int32_t)sj);
-          } else {
-            v = zero_window ? 0 : (uint16_t)(kMarkerBase + kWindow + before + sj);
-          }
-          *page_addr(ph, prel + (int32_t)j) = v;
-        }
-        if (!zero_window) {
-          uint32_t m = __ballot_sync(0xFFFFFFFFu, act && v >= kMarkerBase);
-          if (m) marker_end = o + mo + j0 + 32 - __clz(m);
-        }
-        if (wrap) {
-          r += step_mod;
-          if (r >= dist) r -= dist;
-        }
-      }
+      if (p >= 32) break;
     }
     if (status != kOk) break;
+    const uint32_t kind = (info >> 6) & 3;
+    const bool is_match = on && kind == kKindLen;
+    // a back-reference before the start of the 32 KiB window is invalid
+    if (__any_sync(0xFFFFFFFFu, is_match && (uint64_t)dinfo > o + excl + kWindow)) {
+      status = kBadDeflate;
+      break;
+    }
+    const int32_t orel = (int32_t)(o - (ph.s << 16));  // o within page seq s
+    if (!__any_sync(0xFFFFFFFFu, is_match)) {
+      // literals only: one store each, at their offsets
+      if (on && kind == kKindLit) *page_addr(ph, orel + (int32_t)excl) = (uint16_t)(info >> 16);
+    } else {
+      // The step's entries in passes of 32, lane i writing entry e0 + i: a
+      // literal's value, or a match entry copied from `dist` entries back.
+      // A source before this pass is read from the pages (or is a window
+      // marker / zero before the chunk); a source inside the pass is taken
+      // from its lane by pointer jumping (sources lie strictly below).
+      const uint32_t olen = on ? (kind == kKindLit ? 1u : (kind == kKindLen ? (info >> 16) : 0u)) : 0u;
+      uint8_t* smap = const_cast<uint8_t*>(T->smap);  // the warp's scratch beside its tables
+      uint32_t carry = 0;  // lane of the symbol that covers the pass's first entry
+      for (uint32_t e0 = 0; e0 < acc; e0 += 32) {
+        const bool starts = olen && excl >= e0 && excl < e0 + 32;
+        const uint32_t smask = __reduce_or_sync(0xFFFFFFFFu, starts ? 1u << (excl - e0) : 0u);
+        if (starts) smap[excl - e0] = (uint8_t)lane;
+        __syncwarp();
+        const uint32_t below = smask & (0xFFFFFFFFu >> (31 - lane));
+        const uint32_t L = below ? smap[31 - __clz(below)] : carry;
+        carry = __shfl_sync(0xFFFFFFFFu, L, 31);
+        const uint32_t iL = __shfl_sync(0xFFFFFFFFu, info, (int)L);
+        const uint32_t dL = __shfl_sync(0xFFFFFFFFu, dinfo, (int)L);
+        const uint32_t e = e0 + lane;
+        const bool act = e < acc;
+        uint32_t v = iL >> 16;  // a literal's value
+        int32_t ref = -1;
+        if (act && ((iL >> 6) & 3) == kKindLen) {
+          const int32_t rel = (int32_t)e - (int32_t)dL;  // source, relative to the step start
+          if (rel >= (int32_t)e0) {
+            ref = rel - (int32_t)e0;
+          } else if ((int64_t)o + rel >= 0) {
+            v = *page_addr(ph, orel + rel);
+          } else {
+            v = zero_window ? 0u : (uint32_t)((int64_t)(kMarkerBase + kWindow) + (int64_t)o + rel);
+          }
+        }
+        while (__any_sync(0xFFFFFFFFu, ref >= 0)) {
+          const uint32_t rv = __shfl_sync(0xFFFFFFFFu, v, ref & 31);
+          const int32_t rr = __shfl_sync(0xFFFFFFFFu, ref, ref & 31);
+          if (ref >= 0) {
+            v = rv;
+            ref = rr;
+          }
+        }
+        if (act) *page_addr(ph, orel + (int32_t)e) = (uint16_t)v;
+        if (!zero_window) {
+          const uint32_t m = __ballot_sync(0xFFFFFFFFu, act && v >= kMarkerBase);
+          if (m) marker_end = o + e0 + 32 - __clz(m);
+        }
+        __syncwarp();
+      }
+    }
     __syncwarp();
-    o += step_out;
+    o += acc;
     pos += p;
     if (at_sync) {
       synced = true;
