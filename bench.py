@@ -162,6 +162,9 @@ def bench_batch(args, rank: int, world: int, local: int):
     """Batched path: all streams in one job per step (device-resident input and
     output) against the plain path (one stream per call) on the same GPU."""
     packed, offs, lens, sizes, meta = load_batch(args.scale)
+    if world > 1 and args.impl != "reference":
+        return bench_sharded(args, rank, world, local, "stream_batch", packed, offs, lens, sizes,
+                             meta)
     n = len(offs)
     config = {"workload": "stream_batch", "streams": n, "levels": meta["levels"],
               "seed": 1237, "plain_bytes": meta["plain_bytes"], "comp_bytes": meta["comp_bytes"],
@@ -313,6 +316,87 @@ def bench_batch(args, rank: int, world: int, local: int):
     ctx.close()
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def bench_sharded(args, rank: int, world: int, local: int, name: str, packed, offs, lens,
+                  sizes, meta):
+    """Independent gzip streams across `world` GPUs (the members of the
+    multi-member stream, or the streams of the batch): each rank decodes a
+    disjoint LPT share of them (by compressed size) as one batch job per
+    step; there is no collective on the data path.  The total work is fixed
+    as ranks are added (strong scaling); the job time is the slowest rank's,
+    and every rank's streams must pass their CRC32/ISIZE checks."""
+    import datetime
+    import torch
+    import torch.distributed as dist
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                            device_id=torch.device("cuda", local))
+    torch.cuda.set_device(local)
+    import gzippy_b200 as G
+    mine = lpt_shards(lens, world)[rank]
+    sub_offs = np.zeros(len(mine), np.uint64)
+    at = 0
+    for k, i in enumerate(mine):
+        sub_offs[k] = at
+        at += (int(lens[i]) + 15) & ~15
+    sub = np.zeros(at + 1024, np.uint8)
+    for k, i in enumerate(mine):
+        sub[int(sub_offs[k]):int(sub_offs[k]) + int(lens[i])] = \
+            packed[int(offs[i]):int(offs[i]) + int(lens[i])]
+    sub_lens = np.asarray(lens, np.uint64)[mine]
+    total = int(np.asarray(sizes, np.int64)[mine].sum())
+    ctx = G.Context(device=local)
+    d_in = torch.from_numpy(sub).cuda()
+    d_out = torch.empty(total + 4096, dtype=torch.uint8, device="cuda")
+
+    def step():
+        return ctx.decompress_batch_device(d_in.data_ptr(), sub_offs, sub_lens, d_out.data_ptr(),
+                                           d_out.numel())
+
+    for _ in range(args.warmup):
+        oo, ol, st = step()
+    ok = bool((st == 0).all()) and int(ol.sum()) == total
+    launches = 0
+    with ClockSampler(local) as clk:
+        dist.barrier()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            step()
+            launches += ctx.stats().kernel_launches
+        e1.record()
+        torch.cuda.synchronize()
+        dist.barrier()
+    ms = max_over_ranks(e0.elapsed_time(e1), dist)
+    agg = torch.tensor([float(total), 0.0 if ok else 1.0], dtype=torch.float64, device="cuda")
+    dist.all_reduce(agg)
+    value = args.steps * float(agg[0].item()) / (ms / 1e3) / 1e9
+    ctx.close()
+    if rank == 0:
+        print(json.dumps({
+            "metric": METRIC, "value": round(value, 4), "unit": "GB/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3),
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "u8",
+            "data": "synthetic (seeded generator + zlib levels 1/6/9)",
+            "config": {"workload": name, "streams": len(lens), "plain_bytes": meta["plain_bytes"],
+                       "comp_bytes": meta["comp_bytes"],
+                       "parallelism": f"streams sharded x{world} (LPT by compressed size)",
+                       "l2": "inputs and outputs larger than the 126 MB L2; no flush"},
+            "all_streams_ok": agg[1].item() == 0, "clocks": clk.summary(),
+            "gpu_launches": int(launches)}), flush=True)
+    dist.destroy_process_group()
+
+
+def bench_members_sharded(args, rank: int, world: int, local: int):
+    """The multi-member stream across GPUs: its members are independent gzip
+    streams, sharded like a batch."""
+    comp, meta = load_workload("multi_member", args.scale)
+    mlen = np.array(meta["member_comp_bytes"], np.int64)
+    moff = np.concatenate([[0], np.cumsum(mlen)[:-1]]).astype(np.uint64)
+    sizes = np.full(len(mlen), meta["plain_bytes"] // len(mlen), np.int64)
+    return bench_sharded(args, rank, world, local, "multi_member", comp, moff, mlen, sizes, meta)
 
 
 def run_trace(srv, comps, sizes, crcs, arrivals, free, verify_every: int = 8):
@@ -542,7 +626,8 @@ def committed_traffic(workload: str):
     return d.get("dram_bytes_per_comp_byte")
 
 
-def cpu_baseline(comp: np.ndarray, meta: dict, budget_s: float = 12.0, threads: int | None = None):
+def cpu_baseline(comp: np.ndarray, meta: dict, budget_s: float = 12.0, threads: int | None = None,
+                 scale: float = 1.0):
     """The oracle's chunked speculative decoder on all host threads."""
     from oracle import pyoracle as O
     th = threads or cpus()
@@ -559,7 +644,67 @@ def cpu_baseline(comp: np.ndarray, meta: dict, budget_s: float = 12.0, threads: 
     gbs = meta["plain_bytes"] / statistics.median(times) / 1e9
     return {"value": round(gbs, 3), "unit": "GB/s", "cores": th, "kind": "port",
             "sample": f"{len(times)} full decodes of the {meta['plain_bytes'] >> 20} MiB stream "
-                      f"(oracle chunked decoder, 4 MiB chunks, median)"}
+                      f"(oracle chunked decoder, 4 MiB chunks, median)",
+            "cpu": cpu_model(), "config0": config0_baselines(scale=scale)}
+
+
+def cpu_model() -> str:
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def config0_baselines(budget_s: float = 8.0, scale: float = 1.0) -> dict:
+    """The CPU figures on the 64 MiB Markov-text member (level 6, one serial
+    zlib stream): the oracle's serial decoder on 1 thread (the reference's
+    one-thread loop, chunk_fetcher.rs drive_thin_t1_oracle), its chunked
+    speculative decoder on all host threads, and system zlib's inflate on 1
+    thread (the shape of tools/bench/zng_gunzip.c).  Each is the median of
+    the decodes that fit its share of the budget (at least 2)."""
+    import zlib
+    from oracle import pyoracle as O
+    comp, meta = load_workload("single_member_text", scale)
+    n = meta["plain_bytes"]
+    cb = comp.tobytes()
+    th = cpus()
+
+    def timed(fn, share):
+        times, t_end = [], time.time() + share
+        while len(times) < 2 or (time.time() < t_end and len(times) < 10):
+            t0 = time.perf_counter()
+            size = fn()
+            times.append(time.perf_counter() - t0)
+            assert size == n
+        return round(n / statistics.median(times) / 1e9, 4), len(times)
+
+    one, k1 = timed(lambda: O.decompress(comp, cap=n + 4096)[1].size, budget_s / 3)
+    allt, k2 = timed(lambda: O.decompress_chunked(comp, chunk_bytes=4 << 20, threads=th,
+                                                  cap=n + 4096)[1].size, budget_s / 3)
+    zl, k3 = timed(lambda: len(zlib.decompress(cb, 31)), budget_s / 3)
+    return {"workload": f"single_member_text ({n >> 20} MiB Markov text, level 6, zlib-serial)",
+            "unit": "GB/s", "oracle_1_thread": one, "oracle_all_threads": allt,
+            "threads": th, "zlib_1_thread": zl, "zlib_version": zlib.ZLIB_RUNTIME_VERSION,
+            "decodes": [k1, k2, k3], "cpu": cpu_model()}
+
+
+def lpt_shards(sizes, world: int):
+    """Disjoint work lists for `world` ranks: items in descending size, each
+    to the rank with the least total so far (longest processing time first).
+    Every item lands on exactly one rank, and no rank's total exceeds the
+    mean by more than the largest item.  Returns one sorted index list per
+    rank."""
+    import heapq
+    heap = [(0, r) for r in range(world)]
+    out = [[] for _ in range(world)]
+    for i in sorted(range(len(sizes)), key=lambda k: (-int(sizes[k]), k)):
+        load, r = heapq.heappop(heap)
+        out[r].append(i)
+        heapq.heappush(heap, (load + int(sizes[i]), r))
+    return [sorted(x) for x in out]
 
 
 def max_over_ranks(ms: float, dist, device: str = "cuda") -> float:
@@ -609,6 +754,8 @@ def main():
         return bench_batch(args, rank, world, local)
     if args.workload == "serving":
         return bench_serving(args, rank, world, local)
+    if args.workload == "multi_member" and world > 1 and args.impl != "reference":
+        return bench_members_sharded(args, rank, world, local)
 
     config = {"workload": args.workload, "streams": 1, "level": 6, "seed": 1235,
               "plain_bytes": None, "comp_bytes": None,
@@ -624,7 +771,7 @@ def main():
         th = cpus()
         from oracle import pyoracle as O
         cap = meta["plain_bytes"] + 4096
-        for _ in range(max(1, min(args.warmup, 1))):
+        for _ in range(args.warmup):
             st, out, _ = O.decompress_chunked(comp, chunk_bytes=4 << 20, threads=th, cap=cap)
             assert st == O.OK and out.size == meta["plain_bytes"]
         times = []
@@ -643,7 +790,9 @@ def main():
                 "impl": "reference", "byte_exact": ok,
                 "cpu_baseline": {"value": round(v, 4), "unit": "GB/s", "cores": th, "kind": "port",
                                  "sample": f"{args.steps} full decodes of the whole stream by the "
-                                           "oracle's chunked speculative decoder (4 MiB chunks)"},
+                                           "oracle's chunked speculative decoder (4 MiB chunks)",
+                                 "cpu": cpu_model(),
+                                 "config0": config0_baselines(scale=args.scale)},
                 "e2e": {"value": round(v, 4), "unit": "GB/s", "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
@@ -756,7 +905,7 @@ def main():
                        "tail_marker_chunks": int(st_last.n_tail_marker_chunks),
                        "chunk_bytes": int(st_last.chunk_bytes), "lut_bits": int(st_last.lut_bits)}}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(comp, meta)
+        line["cpu_baseline"] = cpu_baseline(comp, meta, scale=args.scale)
     ctx.close()
     if rank == 0:
         print(json.dumps(line), flush=True)
