@@ -141,18 +141,23 @@ def test_device_raw_and_zlib_high_ratio_grow_the_page_pool():
     formats carry no ISIZE, so the page pool starts at 4x the input, far too
     small: the chunks that run out of pages are decoded again in a grown pool
     (up to deflate's 1032:1 ceiling), and the output is exact."""
+    import ctypes
     import gzippy_b200 as G
     n = 256 << 20
-    cx = G.Context()
-    try:
-        for wbits, fn in ((-15, cx.inflate_raw), (15, cx.inflate_zlib)):
-            comp = _zeros_deflate(n, wbits)
-            assert len(comp) * 500 < n
-            got = fn(comp)
-            assert len(got) == n and got.count(0) == n, wbits
+    for wbits, entry in ((-15, "gzgpu_inflate_raw"), (15, "gzgpu_inflate_zlib")):
+        comp = np.frombuffer(_zeros_deflate(n, wbits), np.uint8)
+        assert comp.size * 500 < n
+        cx = G.Context()          # a fresh pool, sized from the input alone
+        try:
+            out = np.full(n + 64, 0xA5, np.uint8)
+            got = ctypes.c_size_t(0)
+            rc = getattr(cx._lib, entry)(cx._h, comp.ctypes.data, comp.size, out.ctypes.data,
+                                         out.size, ctypes.byref(got))
+            assert rc == G.OK and got.value == n, (entry, rc)
+            assert not out[:n].any() and out[n] == 0xA5
             assert cx.stats().pool_regrows >= 1
-    finally:
-        cx.close()
+        finally:
+            cx.close()
 
 
 @pytest.mark.gpu
