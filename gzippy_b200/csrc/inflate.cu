@@ -905,6 +905,7 @@ __device__ int32_t huff_block_lanes(BitReader& br, const Tables<LB>* T, PageHist
           if (!dead) changed = true;
           dead = true;
         } else if (t != t_used || dead) {
+          if (dead) changed = true;  // revived: the next lane must look again
           dead = false;
           t_used = t;
           uint64_t nx = t;
