@@ -895,7 +895,8 @@ __device__ int32_t huff_block_lanes(BitReader& br, const Tables<LB>* T, PageHist
     uint64_t x = xa, t_used = lane == 0 ? s : kNoStop;
     uint32_t stop = sa;
     bool dead = false;  // past a true stop of an earlier lane
-    for (int round = 0; round <= 32; round++) {
+    bool settled = false;
+    for (int round = 0; round <= 64; round++) {
       const uint64_t t = __shfl_up_sync(FULL, x, 1);
       const uint32_t pstop = __shfl_up_sync(FULL, stop, 1);
       const bool pdead = __shfl_up_sync(FULL, dead ? 1u : 0u, 1) != 0;
@@ -952,7 +953,14 @@ __device__ int32_t huff_block_lanes(BitReader& br, const Tables<LB>* T, PageHist
           stop = ns;
         }
       }
-      if (!__any_sync(FULL, changed)) break;
+      if (!__any_sync(FULL, changed)) {
+        settled = true;
+        break;
+      }
+    }
+    if (!settled) {  // (not reached: a change moves one lane on per round)
+      status = kNotDecoded;
+      break;
     }
     const uint64_t t0 = t_used;  // this lane's true start
     // ---- B: output counts from the true starts, and where the window ends
@@ -1039,7 +1047,10 @@ __device__ int32_t huff_block_lanes(BitReader& br, const Tables<LB>* T, PageHist
       }
       if (kw < 0) kw = 0;  // (lane 0 never overflows: its count stops at kWinOut)
     }
-    (void)alive;
+    if ((~alive & (0xFFFFFFFFu >> (31 - kw))) != 0) {
+      status = kNotDecoded;  // (not reached: a lane past a true stop is never in the window)
+      break;
+    }
     if (wcut == kCutErr) {
       // the true decode reached an invalid code or its read limit
       const uint32_t so = __shfl_sync(FULL, stop, kw);
