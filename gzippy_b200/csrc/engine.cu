@@ -182,7 +182,7 @@ struct gzgpu_ctx {
   bool fine_split = false;  // output-estimate pieces + dynamic-block sync starts
   bool high_priority = false;  // stream at the device's greatest priority
   bool lpt = true;             // decode work list longest-first (else in stream order)
-  bool lanes = true;           // lane-range Huffman decoder (else the 32-bit step decoder)
+  bool lanes = false;          // lane-range Huffman decoder (else the 32-bit step decoder)
   bool job_raw = false;        // the job's streams are raw DEFLATE (no gzip framing)
   bool job_sync = true;     // the running job has sync starts (decoder variant)
   int decode_blocks = 0;
@@ -1328,7 +1328,7 @@ int gzgpu_create(gzgpu_ctx** out, const gzgpu_config* cfg) {
     c->fine_split = cfg->fine_split != 0;
     c->high_priority = cfg->high_priority != 0;
     c->lpt = cfg->work_order == 0;
-    c->lanes = cfg->decoder == 0;
+    c->lanes = cfg->decoder == 1;
   }
   if (cudaSetDevice(c->dev) != cudaSuccess) {
     delete c;
