@@ -776,67 +776,73 @@ constexpr uint32_t kLaneBits = 512;                // input bits per lane and wi
 constexpr uint32_t kLaneWords = kLaneBits / 32;    // the lane's boundary bitmask
 constexpr uint32_t kWinOut = 16384;                // output entries of one window at most
 constexpr uint32_t kLaneFlagWords = kWinOut / 32;  // lane-marker flags (per warp)
+static_assert(kLaneWords * 32 <= kLaneFlagWords, "the boundary bitmasks share the flag words");
 
 enum : uint32_t { kLsNone = 0, kLsEob = 1, kLsBad = 2, kLsLimit = 3 };
 enum : uint32_t { kCutNone = 0, kCutSync = 1, kCutPassed = 2, kCutEob = 3, kCutErr = 4, kCutCap = 5 };
 
-// a lane's own bit reader: buf holds nb >= 33 valid bits after refill()
+// a lane's own bit reader: a 128-bit buffer (lo = bits 0..63 from pos, hi =
+// bits 64..127) that refill() keeps at 48 bits or more, the longest symbol
 struct LaneBits {
   const uint32_t* in32;
-  uint64_t buf, wpos, pos;
+  uint64_t lo, hi, wpos, pos;
   int nb;
   __device__ __forceinline__ void seek(uint64_t p) {
     pos = p;
     wpos = p >> 5;
-    buf = in32[wpos++] >> (p & 31);
+    lo = in32[wpos++] >> (p & 31);
+    hi = 0;
     nb = 32 - (int)(p & 31);
   }
+  __device__ __forceinline__ void append(uint32_t w) {
+    const int b = nb;  // 0..96
+    if (b < 64) lo |= (uint64_t)w << b;
+    if (b > 32) hi |= b >= 64 ? (uint64_t)w << (b - 64) : (uint64_t)w >> (64 - b);
+    nb = b + 32;
+  }
   __device__ __forceinline__ void refill() {
-    if (nb <= 32) {
-      buf |= (uint64_t)in32[wpos++] << nb;
-      nb += 32;
+    if (nb < 48) {
+      append(in32[wpos++]);
+      if (nb < 48) append(in32[wpos++]);
     }
   }
-  __device__ __forceinline__ void consume(uint32_t k) {
-    buf >>= k;
+  __device__ __forceinline__ void consume(uint32_t k) {  // 1 <= k <= 48
+    lo = (lo >> k) | (hi << (64 - k));
+    hi >>= k;
     nb -= (int)k;
     pos += k;
   }
 };
-
 // one symbol at lb.pos with the block's tables: kKindLit (val = byte),
-// kKindLen (val = length, dist), kKindEob or kKindBad
+// kKindLen (val = length, dist), kKindEob or kKindBad.  Both the literal and
+// the length path are computed for every lane (no divergence between them);
+// only codes longer than the lookup tables branch.
 template <int LB>
 __device__ __forceinline__ uint32_t lane_symbol(LaneBits& lb, const Tables<LB>* T, uint32_t& val,
                                                 uint32_t& dist) {
   constexpr uint32_t LMASK = (1u << LB) - 1, DMASK = (1u << kDistBits) - 1;
   lb.refill();
-  uint32_t e = T->lit_lut[lb.buf & LMASK];
+  const uint64_t x = lb.lo;
+  uint32_t e = T->lit_lut[x & LMASK];
   if ((e & 15) == 0) {
-    e = slow_decode<LB>(lb.buf, T->lit_count, T->lit_first, T->lit_offs, T->lit_sorted, litlen_entry);
+    e = slow_decode<LB>(x, T->lit_count, T->lit_first, T->lit_offs, T->lit_sorted, litlen_entry);
     if (e == 0) return kKindBad;
   }
-  const uint32_t L = e & 15, kind = (e >> 8) & 3;
-  if (kind != kKindLen) {
-    val = e >> 16;
-    if (kind != kKindBad) lb.consume(L);
-    return kind;
-  }
-  const uint32_t xb = (e >> 4) & 15;
-  val = (e >> 16) + ((uint32_t)(lb.buf >> L) & ((1u << xb) - 1));
-  lb.consume(L + xb);
-  lb.refill();
-  uint32_t de = T->dist_lut[lb.buf & DMASK];
-  if ((de & 15) == 0) {
-    de = slow_decode<kDistBits>(lb.buf, T->dist_count, T->dist_first, T->dist_offs, T->dist_sorted,
+  const uint32_t L = e & 15, kind = (e >> 8) & 3, xb = (e >> 4) & 15;
+  val = (e >> 16) + ((uint32_t)(x >> L) & ((1u << xb) - 1));
+  const uint32_t sh = L + xb;
+  const uint64_t y = x >> sh;
+  uint32_t de = T->dist_lut[y & DMASK];
+  if (kind == kKindLen && (de & 15) == 0) {
+    de = slow_decode<kDistBits>(y, T->dist_count, T->dist_first, T->dist_offs, T->dist_sorted,
                                 dist_entry);
     if (de == 0) return kKindBad;
   }
-  if (((de >> 8) & 3) == kKindBad) return kKindBad;
   const uint32_t DL = de & 15, dxb = (de >> 4) & 15;
-  dist = (de >> 16) + ((uint32_t)(lb.buf >> DL) & ((1u << dxb) - 1));
-  lb.consume(DL + dxb);
-  return kKindLen;
+  dist = (de >> 16) + ((uint32_t)(y >> DL) & ((1u << dxb) - 1));
+  if (kind == kKindBad || (kind == kKindLen && ((de >> 8) & 3) == kKindBad)) return kKindBad;
+  lb.consume(kind == kKindLen ? sh + DL + dxb : L);
+  return kind;
 }
 
 template <int LB, bool kSync>
@@ -858,9 +864,12 @@ __device__ int32_t huff_block_lanes(BitReader& br, const Tables<LB>* T, PageHist
     }
     // ---- A: speculative decode of each lane's range, boundaries recorded
     const uint64_t s = pos_w + (uint64_t)lane * kLaneBits, e = s + kLaneBits;
-    uint32_t bm[kLaneWords];
+    // this lane's boundary bitmask: word k at bm[k * 32] (the lane's bank),
+    // in the flag words, which the write pass clears and reuses
+    uint32_t* bm = lflags + lane;
+    __syncwarp();
 #pragma unroll
-    for (uint32_t k = 0; k < kLaneWords; k++) bm[k] = 0;
+    for (uint32_t k = 0; k < kLaneWords; k++) bm[k * 32] = 0;
     uint64_t xa = s;  // exit (or stop position) of the decode from s
     uint32_t sa = kLsNone;
     LaneBits lb;
@@ -881,7 +890,7 @@ __device__ int32_t huff_block_lanes(BitReader& br, const Tables<LB>* T, PageHist
           break;
         }
         const uint32_t r = (uint32_t)(p - s);
-        bm[r >> 5] |= 1u << (r & 31);
+        bm[(r >> 5) * 32] |= 1u << (r & 31);
         uint32_t val = 0, dist = 0;
         const uint32_t k = lane_symbol<LB>(lb, T, val, dist);
         if (k == kKindBad || k == kKindEob) {
@@ -915,7 +924,7 @@ __device__ int32_t huff_block_lanes(BitReader& br, const Tables<LB>* T, PageHist
             ns = kLsBad;  // (not reached: a lane's exit is at or past its range end)
           } else if (t >= e) {
             nx = t;  // no symbol starts in this lane's range
-          } else if ((bm[(t - s) >> 5] >> ((t - s) & 31)) & 1) {
+          } else if ((bm[((t - s) >> 5) * 32] >> ((t - s) & 31)) & 1) {
             nx = xa;  // already on the true path
             ns = sa;
           } else if ((t >> 5) + 4 > limit_words) {
@@ -929,7 +938,7 @@ __device__ int32_t huff_block_lanes(BitReader& br, const Tables<LB>* T, PageHist
                 break;
               }
               const uint32_t r = (uint32_t)(p - s);
-              if ((bm[r >> 5] >> (r & 31)) & 1) {
+              if ((bm[(r >> 5) * 32] >> (r & 31)) & 1) {
                 nx = xa;  // joined the recorded path
                 ns = sa;
                 break;
@@ -1071,6 +1080,7 @@ __device__ int32_t huff_block_lanes(BitReader& br, const Tables<LB>* T, PageHist
         status = kPoolExhausted;
         break;
       }
+      __syncwarp();  // every lane is done with its boundary bitmask
       for (uint32_t w = lane; w < (total + 31) / 32; w += 32) lflags[w] = 0;
       __syncwarp();
     }
