@@ -736,8 +736,6 @@ def main():
     ap.add_argument("--lut-bits", type=int, default=0)
     ap.add_argument("--ctas-per-sm", type=int, default=0)
     ap.add_argument("--e2e-steps", type=int, default=0)
-    ap.add_argument("--decoder", default="steps", choices=["steps", "lanes"],
-                    help="Huffman block decoder of the inflate kernel")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--rate", type=float, default=0.0, help="serving: arrivals/s (0 = 60%% of capacity)")
@@ -813,7 +811,7 @@ def main():
     config.update(plain_bytes=meta["plain_bytes"], comp_bytes=meta["comp_bytes"],
                       encoder=meta.get("encoder", "zlib-serial"))
     ctx = G.Context(device=local, chunk_bytes=args.chunk_bytes, lut_bits=args.lut_bits,
-                    ctas_per_sm=args.ctas_per_sm, decoder=args.decoder)
+                    ctas_per_sm=args.ctas_per_sm)
 
     # device-resident buffers (torch only allocates device memory here)
     pad = 1024

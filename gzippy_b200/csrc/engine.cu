@@ -182,7 +182,6 @@ struct gzgpu_ctx {
   bool fine_split = false;  // output-estimate pieces + dynamic-block sync starts
   bool high_priority = false;  // stream at the device's greatest priority
   bool lpt = true;             // decode work list longest-first (else in stream order)
-  bool lanes = false;          // lane-range Huffman decoder (else the 32-bit step decoder)
   bool job_raw = false;        // the job's streams are raw DEFLATE (no gzip framing)
   bool job_sync = true;     // the running job has sync starts (decoder variant)
   int decode_blocks = 0;
@@ -237,15 +236,15 @@ struct gzgpu_ctx {
     stats.decode_passes++;
     switch (lut_bits) {
       case 11:
-        return launch_inflate<11>(ring, ctas_per_sm, job_sync, lanes, cur_in, descs.as<ChunkDesc>(), results.as<ChunkResult>(),
+        return launch_inflate<11>(ring, ctas_per_sm, job_sync, cur_in, descs.as<ChunkDesc>(), results.as<ChunkResult>(),
                                   work.as<uint32_t>(), d_work_count, counters.as<uint32_t>() + 3,
                                   pool, decode_blocks, st);
       case 12:
-        return launch_inflate<12>(ring, ctas_per_sm, job_sync, lanes, cur_in, descs.as<ChunkDesc>(), results.as<ChunkResult>(),
+        return launch_inflate<12>(ring, ctas_per_sm, job_sync, cur_in, descs.as<ChunkDesc>(), results.as<ChunkResult>(),
                                   work.as<uint32_t>(), d_work_count, counters.as<uint32_t>() + 3,
                                   pool, decode_blocks, st);
       default:
-        return launch_inflate<10>(ring, ctas_per_sm, job_sync, lanes, cur_in, descs.as<ChunkDesc>(), results.as<ChunkResult>(),
+        return launch_inflate<10>(ring, ctas_per_sm, job_sync, cur_in, descs.as<ChunkDesc>(), results.as<ChunkResult>(),
                                   work.as<uint32_t>(), d_work_count, counters.as<uint32_t>() + 3,
                                   pool, decode_blocks, st);
     }
@@ -254,9 +253,9 @@ struct gzgpu_ctx {
   int setup_decode_grid() {
     int per_sm = 1;
     switch (lut_bits) {
-      case 11: per_sm = inflate_blocks_per_sm<11>(ring, ctas_per_sm, lanes); break;
-      case 12: per_sm = inflate_blocks_per_sm<12>(ring, ctas_per_sm, lanes); break;
-      default: per_sm = inflate_blocks_per_sm<10>(ring, ctas_per_sm, lanes); break;
+      case 11: per_sm = inflate_blocks_per_sm<11>(ring, ctas_per_sm); break;
+      case 12: per_sm = inflate_blocks_per_sm<12>(ring, ctas_per_sm); break;
+      default: per_sm = inflate_blocks_per_sm<10>(ring, ctas_per_sm); break;
     }
     if (per_sm < 1) per_sm = 1;
     decode_blocks = per_sm * sms;
@@ -1328,7 +1327,6 @@ int gzgpu_create(gzgpu_ctx** out, const gzgpu_config* cfg) {
     c->fine_split = cfg->fine_split != 0;
     c->high_priority = cfg->high_priority != 0;
     c->lpt = cfg->work_order == 0;
-    c->lanes = cfg->decoder == 1;
   }
   if (cudaSetDevice(c->dev) != cudaSuccess) {
     delete c;

@@ -749,437 +749,6 @@ __device__ int32_t huff_block_parallel(BitReader& br, const Tables<LB>* T, PageH
   return status;
 }
 
-
-// ---------------------------------------------------------------------------
-// Huffman block body, one input range per lane (self-synchronising decode).
-//
-// The block is decoded in windows of 32 x kLaneBits input bits.  Lane i
-// decodes serially from bit s_i = start + i * kLaneBits, a guess except for
-// lane 0, recording every symbol start of its range in a bitmask, up to its
-// exit (the first symbol start at or past its range end).  Huffman decoding
-// resynchronises: a lane that starts inside a symbol soon falls onto true
-// symbol boundaries.  Lane i's true start is lane i-1's true exit; if that
-// bit is in lane i's bitmask, lane i's decode from there on was already the
-// true one, else it decodes again from the true start until it reaches a
-// recorded boundary (rounds repeat while exits change).  A second pass counts
-// each lane's output from its true start (prefix sums give output offsets)
-// and finds where the window ends (end of block, the successor's sync start,
-// a bit past the successor's start, the output bound, an error); a third
-// pass writes.  A match whose source lies in an earlier lane's output, not
-// yet written, is written as a lane marker (32768 + index into the 32 KiB
-// before the lane's output, flagged in a shared bitmask); a final pass, lane
-// by lane in order, replaces each lane marker with the entry it names.  The
-// chunk's own window markers (sources before the chunk) are written as in
-// the step decoder and stay for the resolve stage.
-// ---------------------------------------------------------------------------
-constexpr uint32_t kLaneBits = 512;                // input bits per lane and window
-constexpr uint32_t kLaneWords = kLaneBits / 32;    // the lane's boundary bitmask
-constexpr uint32_t kWinOut = 16384;                // output entries of one window at most
-constexpr uint32_t kLaneFlagWords = kWinOut / 32;  // lane-marker flags (per warp)
-static_assert(kLaneWords * 32 <= kLaneFlagWords, "the boundary bitmasks share the flag words");
-
-enum : uint32_t { kLsNone = 0, kLsEob = 1, kLsBad = 2, kLsLimit = 3 };
-enum : uint32_t { kCutNone = 0, kCutSync = 1, kCutPassed = 2, kCutEob = 3, kCutErr = 4, kCutCap = 5 };
-
-// a lane's own bit reader: a 128-bit buffer (lo = bits 0..63 from pos, hi =
-// bits 64..127) that refill() keeps at 48 bits or more, the longest symbol
-struct LaneBits {
-  const uint32_t* in32;
-  uint64_t lo, hi, wpos, pos;
-  int nb;
-  __device__ __forceinline__ void seek(uint64_t p) {
-    pos = p;
-    wpos = p >> 5;
-    lo = in32[wpos++] >> (p & 31);
-    hi = 0;
-    nb = 32 - (int)(p & 31);
-  }
-  __device__ __forceinline__ void append(uint32_t w) {
-    const int b = nb;  // 0..96
-    if (b < 64) lo |= (uint64_t)w << b;
-    if (b > 32) hi |= b >= 64 ? (uint64_t)w << (b - 64) : (uint64_t)w >> (64 - b);
-    nb = b + 32;
-  }
-  __device__ __forceinline__ void refill() {
-    if (nb < 48) {
-      append(in32[wpos++]);
-      if (nb < 48) append(in32[wpos++]);
-    }
-  }
-  __device__ __forceinline__ void consume(uint32_t k) {  // 1 <= k <= 48
-    lo = (lo >> k) | (hi << (64 - k));
-    hi >>= k;
-    nb -= (int)k;
-    pos += k;
-  }
-};
-// one symbol at lb.pos with the block's tables: kKindLit (val = byte),
-// kKindLen (val = length, dist), kKindEob or kKindBad.  Both the literal and
-// the length path are computed for every lane (no divergence between them);
-// only codes longer than the lookup tables branch.
-template <int LB>
-__device__ __forceinline__ uint32_t lane_symbol(LaneBits& lb, const Tables<LB>* T, uint32_t& val,
-                                                uint32_t& dist) {
-  constexpr uint32_t LMASK = (1u << LB) - 1, DMASK = (1u << kDistBits) - 1;
-  lb.refill();
-  const uint64_t x = lb.lo;
-  uint32_t e = T->lit_lut[x & LMASK];
-  if ((e & 15) == 0) {
-    e = slow_decode<LB>(x, T->lit_count, T->lit_first, T->lit_offs, T->lit_sorted, litlen_entry);
-    if (e == 0) return kKindBad;
-  }
-  const uint32_t L = e & 15, kind = (e >> 8) & 3, xb = (e >> 4) & 15;
-  val = (e >> 16) + ((uint32_t)(x >> L) & ((1u << xb) - 1));
-  const uint32_t sh = L + xb;
-  const uint64_t y = x >> sh;
-  uint32_t de = T->dist_lut[y & DMASK];
-  if (kind == kKindLen && (de & 15) == 0) {
-    de = slow_decode<kDistBits>(y, T->dist_count, T->dist_first, T->dist_offs, T->dist_sorted,
-                                dist_entry);
-    if (de == 0) return kKindBad;
-  }
-  const uint32_t DL = de & 15, dxb = (de >> 4) & 15;
-  dist = (de >> 16) + ((uint32_t)(y >> DL) & ((1u << dxb) - 1));
-  if (kind == kKindBad || (kind == kKindLen && ((de >> 8) & 3) == kKindBad)) return kKindBad;
-  lb.consume(kind == kKindLen ? sh + DL + dxb : L);
-  return kind;
-}
-
-template <int LB, bool kSync>
-__device__ int32_t huff_block_lanes(BitReader& br, const Tables<LB>* T, PageHist& ph,
-                                    const PagePool& pool, uint32_t cid, uint32_t gen, uint64_t& o,
-                                    uint64_t& guard, uint64_t& marker_end, bool zero_window,
-                                    uint64_t trunc_words, uint64_t sync_target, uint64_t passed_bit,
-                                    bool& synced, bool& passed, uint32_t* lflags, int lane) {
-  const uint32_t FULL = 0xFFFFFFFFu;
-  const uint32_t* in32 = br.in32;
-  const uint64_t limit_words = br.limit_words;
-  uint64_t pos_w = br.pos();  // window start: a true symbol boundary
-  int32_t status = kOk;
-  guard = 0;
-  for (;;) {
-    if (kSync && sync_target == pos_w) {
-      synced = true;
-      break;
-    }
-    // ---- A: speculative decode of each lane's range, boundaries recorded
-    const uint64_t s = pos_w + (uint64_t)lane * kLaneBits, e = s + kLaneBits;
-    // this lane's boundary bitmask: word k at bm[k * 32] (the lane's bank),
-    // in the flag words, which the write pass clears and reuses
-    uint32_t* bm = lflags + lane;
-    __syncwarp();
-#pragma unroll
-    for (uint32_t k = 0; k < kLaneWords; k++) bm[k * 32] = 0;
-    uint64_t xa = s;  // exit (or stop position) of the decode from s
-    uint32_t sa = kLsNone;
-    LaneBits lb;
-    lb.in32 = in32;
-    if ((s >> 5) + 4 > limit_words) {
-      sa = kLsLimit;
-    } else {
-      lb.seek(s);
-      for (;;) {
-        const uint64_t p = lb.pos;
-        if (p >= e) {
-          xa = p;
-          break;
-        }
-        if ((p >> 5) + 4 > limit_words) {
-          sa = kLsLimit;
-          xa = p;
-          break;
-        }
-        const uint32_t r = (uint32_t)(p - s);
-        bm[(r >> 5) * 32] |= 1u << (r & 31);
-        uint32_t val = 0, dist = 0;
-        const uint32_t k = lane_symbol<LB>(lb, T, val, dist);
-        if (k == kKindBad || k == kKindEob) {
-          sa = k == kKindBad ? kLsBad : kLsEob;
-          xa = p;
-          break;
-        }
-      }
-    }
-    // ---- sync: true starts, rounds until no exit changes
-    uint64_t x = xa, t_used = lane == 0 ? s : kNoStop;
-    uint32_t stop = sa;
-    bool dead = false;  // past a true stop of an earlier lane
-    bool settled = false;
-    for (int round = 0; round <= 64; round++) {
-      const uint64_t t = __shfl_up_sync(FULL, x, 1);
-      const uint32_t pstop = __shfl_up_sync(FULL, stop, 1);
-      const bool pdead = __shfl_up_sync(FULL, dead ? 1u : 0u, 1) != 0;
-      bool changed = false;
-      if (lane > 0) {
-        if (pdead || pstop != kLsNone) {
-          if (!dead) changed = true;
-          dead = true;
-        } else if (t != t_used || dead) {
-          if (dead) changed = true;  // revived: the next lane must look again
-          dead = false;
-          t_used = t;
-          uint64_t nx = t;
-          uint32_t ns = kLsNone;
-          if (t < s) {
-            ns = kLsBad;  // (not reached: a lane's exit is at or past its range end)
-          } else if (t >= e) {
-            nx = t;  // no symbol starts in this lane's range
-          } else if ((bm[((t - s) >> 5) * 32] >> ((t - s) & 31)) & 1) {
-            nx = xa;  // already on the true path
-            ns = sa;
-          } else if ((t >> 5) + 4 > limit_words) {
-            ns = kLsLimit;
-          } else {
-            lb.seek(t);
-            for (;;) {
-              const uint64_t p = lb.pos;
-              if (p >= e) {
-                nx = p;
-                break;
-              }
-              const uint32_t r = (uint32_t)(p - s);
-              if ((bm[(r >> 5) * 32] >> (r & 31)) & 1) {
-                nx = xa;  // joined the recorded path
-                ns = sa;
-                break;
-              }
-              if ((p >> 5) + 4 > limit_words) {
-                ns = kLsLimit;
-                nx = p;
-                break;
-              }
-              uint32_t val = 0, dist = 0;
-              const uint32_t k = lane_symbol<LB>(lb, T, val, dist);
-              if (k == kKindBad || k == kKindEob) {
-                ns = k == kKindBad ? kLsBad : kLsEob;
-                nx = p;
-                break;
-              }
-            }
-          }
-          if (nx != x || ns != stop) changed = true;
-          x = nx;
-          stop = ns;
-        }
-      }
-      if (!__any_sync(FULL, changed)) {
-        settled = true;
-        break;
-      }
-    }
-    if (!settled) {  // (not reached: a change moves one lane on per round)
-      status = kNotDecoded;
-      break;
-    }
-    const uint64_t t0 = t_used;  // this lane's true start
-    // ---- B: output counts from the true starts, and where the window ends
-    uint32_t cnt = 0, cut = kCutNone;
-    uint64_t end = x, eob_end = 0;
-    if (!dead) {
-      if ((t0 >> 5) + 4 > limit_words) {
-        cut = kCutErr;
-        end = t0;
-      } else {
-        lb.seek(t0);
-        for (;;) {
-          const uint64_t p = lb.pos;
-          if (kSync && p == sync_target) {
-            cut = kCutSync;
-            end = p;
-            break;
-          }
-          if (kSync && p > passed_bit && p > pos_w) {
-            cut = kCutPassed;
-            end = p;
-            break;
-          }
-          if (stop != kLsNone && p == x) {
-            end = p;
-            if (stop == kLsEob) {
-              uint32_t val = 0, dist = 0;
-              lane_symbol<LB>(lb, T, val, dist);
-              eob_end = lb.pos;
-              cut = kCutEob;
-            } else {
-              cut = kCutErr;
-            }
-            break;
-          }
-          if (p >= e) {
-            end = p;
-            break;
-          }
-          uint32_t val = 0, dist = 0;
-          const uint32_t k = lane_symbol<LB>(lb, T, val, dist);
-          if (k == kKindBad || k == kKindEob) {  // (not reached: the sync pass found the stops)
-            stop = kLsBad;
-            cut = kCutErr;
-            end = p;
-            break;
-          }
-          const uint32_t n = k == kKindLit ? 1u : val;
-          if (cnt + n > kWinOut) {
-            cut = kCutCap;
-            end = p;
-            break;
-          }
-          cnt += n;
-        }
-      }
-    }
-    // the window: lanes up to the first cut, within kWinOut entries
-    uint32_t incl = cnt;
-#pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-      const uint32_t v = __shfl_up_sync(FULL, incl, d);
-      if (lane >= d) incl += v;
-    }
-    const uint32_t off = incl - cnt;
-    const uint32_t over = __ballot_sync(FULL, !dead && off + cnt > kWinOut);
-    const uint32_t cuts = __ballot_sync(FULL, !dead && cut != kCutNone);
-    const uint32_t alive = __ballot_sync(FULL, !dead);
-    // (a lane past a true stop is dead; the stopping lane has a cut, so the
-    // first cut always comes before any dead lane)
-    int kw;  // last lane in the window
-    uint32_t wcut = kCutNone;
-    {
-      const int k_over = over ? __ffs(over) - 1 : 32;
-      const int k_cut = cuts ? __ffs(cuts) - 1 : 32;
-      const uint32_t cut_k = __shfl_sync(FULL, cut, k_cut & 31);
-      if (k_over <= k_cut) {
-        kw = k_over - 1;  // the window ends before the lane whose output would overflow it
-      } else if (cut_k == kCutCap && k_cut > 0) {
-        kw = k_cut - 1;   // a lane that alone overflows starts the next window
-      } else {
-        kw = k_cut;
-        wcut = cut_k;
-      }
-      if (kw < 0) kw = 0;  // (lane 0 never overflows: its count stops at kWinOut)
-    }
-    if ((~alive & (0xFFFFFFFFu >> (31 - kw))) != 0) {
-      status = kNotDecoded;  // (not reached: a lane past a true stop is never in the window)
-      break;
-    }
-    if (wcut == kCutErr) {
-      // the true decode reached an invalid code or its read limit
-      const uint32_t so = __shfl_sync(FULL, stop, kw);
-      const uint64_t ep = __shfl_sync(FULL, end, kw);
-      if (so == kLsBad) status = kBadDeflate;
-      else status = (ep >> 5) + 4 > trunc_words ? kTruncated : kOvershoot;
-      pos_w = ep;
-      break;
-    }
-    const uint32_t total = __shfl_sync(FULL, incl, kw);
-    const uint64_t end_bit = wcut == kCutEob ? __shfl_sync(FULL, eob_end, kw)
-                                             : __shfl_sync(FULL, end, kw);
-    const bool in_win = lane <= kw;
-    // ---- C: write, lane by lane in parallel
-    if (total) {
-      ph.advance(o);
-      if (!ph.ensure(pool, cid, gen, o + total, lane)) {
-        status = kPoolExhausted;
-        break;
-      }
-      __syncwarp();  // every lane is done with its boundary bitmask
-      for (uint32_t w = lane; w < (total + 31) / 32; w += 32) lflags[w] = 0;
-      __syncwarp();
-    }
-    const int32_t orel = (int32_t)(o - (ph.s << 16));  // o within page seq s
-    bool bad = false, has_lm = false;
-    uint64_t cm_end = 0;  // 1 + last chunk marker written
-    if (in_win && cnt) {
-      lb.seek(t0);
-      const uint32_t q0 = off;  // window-relative output of this lane
-      uint32_t q = off;
-      while (lb.pos < end) {
-        uint32_t val = 0, dist = 0;
-        const uint32_t k = lane_symbol<LB>(lb, T, val, dist);
-        if (k == kKindLit && q < q0 + cnt) {
-          *page_addr(ph, orel + (int32_t)q) = (uint16_t)val;
-          q++;
-          continue;
-        }
-        // (the count pass decoded the same symbols: a write past it cannot happen)
-        if (k != kKindLen || q + val > q0 + cnt || (uint64_t)dist > o + q + kWindow) {
-          bad = true;
-          break;
-        }
-        for (uint32_t j = 0; j < val; j++, q++) {
-          const int64_t src = (int64_t)q - (int64_t)dist;  // window-relative source
-          uint32_t v;
-          bool fl = false;
-          if (src < (int64_t)q0) {
-            if (src >= 0) {
-              v = kMarkerBase + (uint32_t)(src - ((int64_t)q0 - (int64_t)kWindow));
-              fl = true;
-            } else if ((int64_t)o + src >= 0) {
-              v = *page_addr(ph, orel + (int32_t)src);
-              if (v >= kMarkerBase) cm_end = o + q + 1;
-            } else {
-              v = zero_window ? 0u : (uint32_t)((int64_t)(kMarkerBase + kWindow) + (int64_t)o + src);
-              if (!zero_window) cm_end = o + q + 1;
-            }
-          } else {
-            v = *page_addr(ph, orel + (int32_t)src);
-            fl = (lflags[src >> 5] >> (src & 31)) & 1;
-            if (!fl && v >= kMarkerBase) cm_end = o + q + 1;
-          }
-          *page_addr(ph, orel + (int32_t)q) = (uint16_t)v;
-          if (fl) {
-            atomicOr(&lflags[q >> 5], 1u << (q & 31));
-            has_lm = true;
-          }
-        }
-      }
-    }
-    __syncwarp();
-    if (__any_sync(FULL, bad)) {
-      status = kBadDeflate;
-      break;
-    }
-    // ---- D: lane markers, lane after lane
-    uint32_t lm = __ballot_sync(FULL, in_win && has_lm);
-    while (lm) {
-      const int j = __ffs(lm) - 1;
-      lm &= lm - 1;
-      const uint32_t jo = __shfl_sync(FULL, off, j), jn = __shfl_sync(FULL, cnt, j);
-      for (uint32_t e0 = 0; e0 < jn; e0 += 32) {
-        const uint32_t q = jo + e0 + lane;
-        if (e0 + lane < jn && ((lflags[q >> 5] >> (q & 31)) & 1)) {
-          const uint32_t v = *page_addr(ph, orel + (int32_t)q);
-          // a lane marker names an entry in [jo - 32768, jo), inside the window
-          const int32_t ref = (int32_t)jo - (int32_t)kWindow + (int32_t)(v - kMarkerBase);
-          if (v < kMarkerBase || ref < 0) continue;
-          const uint32_t v2 = *page_addr(ph, orel + ref);
-          *page_addr(ph, orel + (int32_t)q) = (uint16_t)v2;
-          if (v2 >= kMarkerBase) cm_end = max(cm_end, o + q + 1);
-        }
-      }
-      __syncwarp();
-    }
-    if (!zero_window) {
-      uint64_t me = cm_end;
-#pragma unroll
-      for (int d = 16; d >= 1; d >>= 1) me = max(me, __shfl_xor_sync(FULL, me, d));
-      if (me > marker_end) marker_end = me;
-    }
-    o += total;
-    pos_w = end_bit;
-    if (wcut == kCutEob) break;
-    if (kSync && wcut == kCutSync) {
-      synced = true;
-      break;
-    }
-    if (kSync && wcut == kCutPassed) {
-      passed = true;
-      break;
-    }
-  }
-  br.seek(pos_w, lane);
-  br.refill(lane);
-  return status;
-}
-
 // ---------------------------------------------------------------------------
 // Decode one chunk.  kRing selects the history layout.
 // ---------------------------------------------------------------------------
@@ -1188,11 +757,11 @@ __device__ __forceinline__ uint64_t handover_bit(const ChunkDesc& k) {
   return (k.flags & kChunkMemberFirst) ? k.limit_bit * 8 : k.lo_bit;
 }
 
-template <int LB, bool kRing, bool kSync, bool kLanes = false>
+template <int LB, bool kRing, bool kSync>
 __device__ int32_t decode_chunk(const uint8_t* __restrict__ in, ChunkDesc d,
                                 const ChunkDesc* descs, ChunkResult* res, uint32_t cid,
                                 uint32_t gen, uint16_t* ring, Tables<LB>* T,
-                                const PagePool& pool, int lane, uint32_t* lflags = nullptr) {
+                                const PagePool& pool, int lane) {
   const bool zero_window = (d.flags & kChunkMemberFirst) != 0;
   if (kRing) {
     // seed the ring: zeros for a member start, marker values otherwise
@@ -1421,14 +990,9 @@ __device__ int32_t decode_chunk(const uint8_t* __restrict__ in, ChunkDesc d,
             passed_bit = ((const volatile ChunkDesc*)(descs + d.next))->start_bit;
         }
         bool passed = false;
-        if constexpr (kLanes)
-          status = huff_block_lanes<LB, kSync>(br, T, ph, pool, cid, gen, o, guard, marker_end,
-                                               zero_window, trunc_words, sync_target, passed_bit,
-                                               synced, passed, lflags, lane);
-        else
-          status = huff_block_parallel<LB, kSync>(br, T, ph, pool, cid, gen, o, guard, marker_end,
-                                                  zero_window, trunc_words, sync_target, passed_bit,
-                                                  synced, passed, lane);
+        status = huff_block_parallel<LB, kSync>(br, T, ph, pool, cid, gen, o, guard, marker_end,
+                                         zero_window, trunc_words, sync_target, passed_bit, synced,
+                                         passed, lane);
         if (status != kOk || synced) break;
         if (passed) {
           extend(descs[d.next].next);
@@ -1598,12 +1162,12 @@ __device__ int32_t decode_chunk(const uint8_t* __restrict__ in, ChunkDesc d,
 
 // Work loop shared by both kernels: take chunks from the queue; a failed
 // speculative start moves on to the next candidate of its partition.
-template <int LB, bool kRing, bool kSync, bool kLanes = false>
+template <int LB, bool kRing, bool kSync>
 __device__ __forceinline__ void work_loop(const uint8_t* __restrict__ in, ChunkDesc* descs,
                                           ChunkResult* results, const uint32_t* work,
                                           uint32_t n_work, uint32_t* work_counter,
                                           const PagePool& pool, uint16_t* ring, Tables<LB>* T,
-                                          int lane, uint32_t* lflags = nullptr) {
+                                          int lane) {
   for (;;) {
     uint32_t w = 0;
     if (lane == 0) w = atomicAdd(work_counter, 1u);
@@ -1619,8 +1183,8 @@ __device__ __forceinline__ void work_loop(const uint8_t* __restrict__ in, ChunkD
     // again after the page pool ran out tags its pages past the old ones)
     const uint32_t gen0 = d.flags >> kGenBaseShift;
     for (uint32_t gen = gen0;; gen++) {
-      int32_t st = decode_chunk<LB, kRing, kSync, kLanes>(in, d, descs, &results[cid], cid, gen, ring,
-                                                          T, pool, lane, lflags);
+      int32_t st = decode_chunk<LB, kRing, kSync>(in, d, descs, &results[cid], cid, gen, ring, T, pool,
+                                           lane);
       if (st == kOk || st == kPoolExhausted || !speculative || gen + 1 >= gen0 + kMaxTries) break;
       uint64_t lo = 0, hi = 0;
       if (!warp_find_first(in, d.in_end, d.lo_bit + 1, d.limit_bit, d.limit_bit, lane, lo, hi)) break;
@@ -1654,9 +1218,7 @@ __global__ void __launch_bounds__(32 * kRingWarps)
                             &S->t, lane);
 }
 
-// kLanes: Huffman block bodies by the lane-range decoder (huff_block_lanes),
-// else by the 32-bit step decoder (huff_block_parallel)
-template <int LB, int MINB, bool kSync, bool kLanes>
+template <int LB, int MINB, bool kSync>
 __global__ void __launch_bounds__(32 * kPageWarps, MINB)
     inflate_pages_kernel(const uint8_t* __restrict__ in, ChunkDesc* __restrict__ descs,
                          ChunkResult* __restrict__ results, const uint32_t* __restrict__ work,
@@ -1665,40 +1227,32 @@ __global__ void __launch_bounds__(32 * kPageWarps, MINB)
   extern __shared__ __align__(16) uint8_t smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   Tables<LB>* T = reinterpret_cast<Tables<LB>*>(smem) + warp;
-  uint32_t* lflags = kLanes ? reinterpret_cast<uint32_t*>(
-                                  smem + sizeof(Tables<LB>) * kPageWarps) + warp * kLaneFlagWords
-                            : nullptr;
-  work_loop<LB, false, kSync, kLanes>(in, descs, results, work, *n_work_ptr, work_counter, pool,
-                                      nullptr, T, lane, lflags);
+  work_loop<LB, false, kSync>(in, descs, results, work, *n_work_ptr, work_counter, pool, nullptr,
+                              T, lane);
 }
 
 template <int LB>
-size_t inflate_smem_bytes(bool ring, bool lanes) {
-  return ring ? sizeof(RingSmem<LB>) * kRingWarps
-              : (sizeof(Tables<LB>) + (lanes ? 4 * kLaneFlagWords : 0)) * kPageWarps;
+size_t inflate_smem_bytes(bool ring) {
+  return ring ? sizeof(RingSmem<LB>) * kRingWarps : sizeof(Tables<LB>) * kPageWarps;
 }
 
 // page kernel instance for `ctas` CTAs per SM (registers sized for it), with
-// or without sync-start support, with the lane-range or the step decoder
-template <int LB, bool kLanes>
-static const void* pages_kernel_fn2(int ctas, bool sync) {
-  if (sync)
-    return ctas >= 4 ? (const void*)inflate_pages_kernel<LB, 4, true, kLanes>
-                     : (const void*)inflate_pages_kernel<LB, 3, true, kLanes>;
-  return ctas >= 4 ? (const void*)inflate_pages_kernel<LB, 4, false, kLanes>
-                   : (const void*)inflate_pages_kernel<LB, 3, false, kLanes>;
-}
+// or without sync-start support
 template <int LB>
-static const void* pages_kernel_fn(int ctas, bool sync, bool lanes) {
-  return lanes ? pages_kernel_fn2<LB, true>(ctas, sync) : pages_kernel_fn2<LB, false>(ctas, sync);
+static const void* pages_kernel_fn(int ctas, bool sync) {
+  if (sync)
+    return ctas >= 4 ? (const void*)inflate_pages_kernel<LB, 4, true>
+                     : (const void*)inflate_pages_kernel<LB, 3, true>;
+  return ctas >= 4 ? (const void*)inflate_pages_kernel<LB, 4, false>
+                   : (const void*)inflate_pages_kernel<LB, 3, false>;
 }
 
 template <int LB>
-cudaError_t launch_inflate(bool ring, int ctas, bool sync, bool lanes, const uint8_t* in,
-                           ChunkDesc* descs, ChunkResult* results, const uint32_t* work,
-                           const uint32_t* n_work, uint32_t* work_counter, const PagePool& pool,
-                           int blocks, cudaStream_t stream) {
-  size_t smem = inflate_smem_bytes<LB>(ring, lanes);
+cudaError_t launch_inflate(bool ring, int ctas, bool sync, const uint8_t* in, ChunkDesc* descs,
+                           ChunkResult* results, const uint32_t* work, const uint32_t* n_work,
+                           uint32_t* work_counter, const PagePool& pool, int blocks,
+                           cudaStream_t stream) {
+  size_t smem = inflate_smem_bytes<LB>(ring);
   cudaError_t e;
   if (ring) {
     e = cudaFuncSetAttribute(inflate_ring_kernel<LB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1707,7 +1261,7 @@ cudaError_t launch_inflate(bool ring, int ctas, bool sync, bool lanes, const uin
     inflate_ring_kernel<LB><<<blocks, 32 * kRingWarps, smem, stream>>>(in, descs, results, work,
                                                                        n_work, work_counter, pool);
   } else {
-    const void* fn = pages_kernel_fn<LB>(ctas, sync, lanes);
+    const void* fn = pages_kernel_fn<LB>(ctas, sync);
     e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     void* args[] = {(void*)&in,   (void*)&descs,        (void*)&results, (void*)&work,
@@ -1719,35 +1273,31 @@ cudaError_t launch_inflate(bool ring, int ctas, bool sync, bool lanes, const uin
 }
 
 template <int LB>
-int inflate_blocks_per_sm(bool ring, int ctas, bool lanes) {
+int inflate_blocks_per_sm(bool ring, int ctas) {
   int n = 0;
-  size_t smem = inflate_smem_bytes<LB>(ring, lanes);
+  size_t smem = inflate_smem_bytes<LB>(ring);
   if (ring) {
     cudaFuncSetAttribute(inflate_ring_kernel<LB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)smem);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, inflate_ring_kernel<LB>, 32 * kRingWarps, smem);
   } else {
-    // the sync and no-sync variants are sized for the same registers; take
-    // the smaller occupancy of the two
-    int n2 = 0;
-    const void* fn = pages_kernel_fn<LB>(ctas, true, lanes);
+    // both variants are sized for the same registers; take the larger
+    const void* fn = pages_kernel_fn<LB>(ctas, true);
     cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, 32 * kPageWarps, smem);
-    const void* fn2 = pages_kernel_fn<LB>(ctas, false, lanes);
-    cudaFuncSetAttribute(fn2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n2, fn2, 32 * kPageWarps, smem);
-    if (n2 < n) n = n2;
+    cudaFuncSetAttribute(pages_kernel_fn<LB>(ctas, false), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)smem);
     if (n > ctas) n = ctas;
   }
   return n;
 }
 
 #define GZGPU_INST(LB)                                                                       \
-  template size_t inflate_smem_bytes<LB>(bool, bool);                                        \
-  template int inflate_blocks_per_sm<LB>(bool, int, bool);                                   \
-  template cudaError_t launch_inflate<LB>(bool, int, bool, bool, const uint8_t*, ChunkDesc*,  \
-                                          ChunkResult*, const uint32_t*, const uint32_t*,    \
-                                          uint32_t*, const PagePool&, int, cudaStream_t);
+  template size_t inflate_smem_bytes<LB>(bool);                                              \
+  template int inflate_blocks_per_sm<LB>(bool, int);                                         \
+  template cudaError_t launch_inflate<LB>(bool, int, bool, const uint8_t*, ChunkDesc*, ChunkResult*, \
+                                          const uint32_t*, const uint32_t*, uint32_t*,       \
+                                          const PagePool&, int, cudaStream_t);
 GZGPU_INST(10)
 GZGPU_INST(11)
 GZGPU_INST(12)

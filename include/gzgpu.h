@@ -72,10 +72,6 @@ typedef struct {
                          contexts' streams (running blocks are not preempted) */
   int work_order;     /* order in which the persistent decoder takes chunks: 0 = longest
                          expected decode first (default), 1 = in stream order */
-  int decoder;        /* Huffman block decoder of the page-history kernel: 0 = 32-bit steps
-                         (all lanes decode candidates at every bit of a step; default),
-                         1 = lane ranges (each lane decodes its own input range; lanes
-                         resynchronise) */
 } gzgpu_config;
 
 typedef struct {
