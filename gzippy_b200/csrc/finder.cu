@@ -46,12 +46,25 @@ __global__ void __launch_bounds__(kStoredThreads)
   if (threadIdx.x == 0) *s_off = ~0ull;
   __syncthreads();
   const uint64_t until = nbytes >= 5 ? min((to + 7) / 8, nbytes - 4) : 0;
-  for (uint64_t base = max((from + 3 + 7) / 8, (uint64_t)2); base < until; base += blockDim.x) {
-    const uint64_t off = base + threadIdx.x;
-    uint64_t lo = 0, hi = 0;
-    if (off < until && stored_candidate(in, nbytes, off, from, to, to, lo, hi) &&
-        stored_successor_ok(in, nbytes, off + 4 + (in[off] | (in[off + 1] << 8))))
-      atomicMin(s_off, (unsigned long long)off);
+  const uint32_t* in32 = reinterpret_cast<const uint32_t*>(in);
+  // each thread screens 4 consecutive byte offsets a round for LEN == ~NLEN
+  for (uint64_t base = max((from + 3 + 7) / 8, (uint64_t)2); base < until; base += 4 * blockDim.x) {
+    const uint64_t ob = base + 4 * (uint64_t)threadIdx.x;
+    uint32_t m = 0;
+    if (ob < until) {
+      m = stored_filter4(bits64_at(in32, ob * 8));
+      if (ob + 4 > until) m &= (1u << (until - ob)) - 1;
+    }
+    while (m) {
+      const uint64_t off = ob + (uint64_t)(__ffs(m) - 1);
+      m &= m - 1;
+      uint64_t lo = 0, hi = 0;
+      if (stored_candidate(in, nbytes, off, from, to, to, lo, hi) &&
+          stored_successor_ok(in, nbytes, off + 4 + (in[off] | (in[off + 1] << 8)))) {
+        atomicMin(s_off, (unsigned long long)off);
+        break;
+      }
+    }
     __syncthreads();
     const bool found = *s_off != ~0ull;
     __syncthreads();  // every thread has read it before the next round writes

@@ -268,18 +268,51 @@ static __device__ __forceinline__ bool stored_candidate(const uint8_t* in, uint6
   return lo >= from && lo < to && hi < hi_to && len != 0 && off + 4 + len <= nbytes;
 }
 
+// Bits [p, p + 64) of the stream from three aligned 32-bit loads (the buffer
+// is padded past the stream; bits past its end are not masked here).
+static __device__ __forceinline__ uint64_t bits64_at(const uint32_t* in32, uint64_t p) {
+  const uint64_t wi = p >> 5;
+  const int sh = (int)(p & 31);
+  const uint64_t a = ((uint64_t)in32[wi + 1] << 32) | in32[wi];
+  return sh ? (a >> sh) | ((uint64_t)in32[wi + 2] << (64 - sh)) : a;
+}
+
+// Positions i < 32 (bit i of the result) where the 13-bit dynamic header
+// filter passes, for the 64 stream bits X starting at the first of them:
+// BFINAL = 0, BTYPE = 10, HLIT <= 29 (not bits 4..7 all set), HDIST <= 29
+// (not bits 9..12 all set).  All 32 positions at once, bit-parallel.
+static __device__ __forceinline__ uint32_t dyn_filter32(uint64_t X) {
+  const uint64_t hlit_big = (X >> 4) & (X >> 5) & (X >> 6) & (X >> 7);
+  const uint64_t hdist_big = (X >> 9) & (X >> 10) & (X >> 11) & (X >> 12);
+  return (uint32_t)(~X & ~(X >> 1) & (X >> 2) & ~hlit_big & ~hdist_big);
+}
+
+// Byte offsets k < 4 (bit k) among off .. off + 3 where LEN == ~NLEN, from
+// the 7 bytes at off held in the low bits of B (bytes beyond are ignored).
+static __device__ __forceinline__ uint32_t stored_filter4(uint64_t B) {
+  uint32_t m = 0;
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    const uint32_t sz = (uint32_t)(B >> (8 * k));
+    m |= (((sz ^ (sz >> 16)) & 0xFFFFu) == 0xFFFFu ? 1u : 0u) << k;
+  }
+  return m;
+}
+
 // First candidate in (bit_offset, seek_bit) order with bit_offset in
 // [from, to) of the stream ending at byte `nbytes` (a stored candidate's
 // seek bit must also be below hi_to); all 32 lanes call it together and get
-// the same answer.  The range is walked in 1024-bit
-// windows; in each, lanes test 32 byte offsets (stored) or 32 bit offsets
-// (dynamic) per step and a ballot picks the lowest hit.  The first stored hit
-// in byte order is the smallest stored candidate, so the dynamic scan only
-// needs to reach it.
+// the same answer.  The range is walked in 1024-bit windows.  In each, every
+// lane first screens 4 byte offsets for a stored block's LEN/NLEN pair, then
+// 32 bit offsets with the 13-bit dynamic header filter, both bit-parallel,
+// and runs the full tests only on the offsets that pass (about 1 in 9 bits);
+// a ballot picks the lowest hit.  The first stored hit in byte order is the
+// smallest stored candidate, so the dynamic scan only needs to reach it.
 static __device__ bool warp_find_first(const uint8_t* __restrict__ in, uint64_t nbytes,
                                        uint64_t from, uint64_t to, uint64_t hi_to, int lane,
                                        uint64_t& out_lo, uint64_t& out_hi,
                                        const uint16_t* leaf_lut = nullptr) {
+  const uint32_t* in32 = reinterpret_cast<const uint32_t*>(in);
   if (to > nbytes * 8) to = nbytes * 8;
   if (hi_to > nbytes * 8) hi_to = nbytes * 8;
   bool have = false;
@@ -291,28 +324,54 @@ static __device__ bool warp_find_first(const uint8_t* __restrict__ in, uint64_t 
     // stored offsets whose candidate may start below w1 (start >= off*8 - 10)
     const uint64_t off_end = min(until, (w1 + 10) / 8 + 1);
     while (!have && next_off < off_end) {
-      uint64_t off = next_off + lane;
+      const uint64_t ob = next_off + 4 * (uint64_t)lane;
+      uint32_t m = 0;
+      if (ob < off_end) {
+        m = stored_filter4(bits64_at(in32, ob * 8));
+        if (ob + 4 > off_end) m &= (1u << (off_end - ob)) - 1;
+      }
       uint64_t lo = 0, hi = 0;
-      bool hit = off < off_end && stored_candidate(in, nbytes, off, from, to, hi_to, lo, hi);
-      uint32_t m = __ballot_sync(0xFFFFFFFFu, hit);
-      if (m) {
-        int src = __ffs(m) - 1;
+      bool hit = false;
+      while (m) {
+        const int k = __ffs(m) - 1;
+        m &= m - 1;
+        if (stored_candidate(in, nbytes, ob + k, from, to, hi_to, lo, hi)) {
+          hit = true;
+          break;
+        }
+      }
+      const uint32_t b = __ballot_sync(0xFFFFFFFFu, hit);
+      if (b) {
+        const int src = __ffs(b) - 1;
         best_lo = __shfl_sync(0xFFFFFFFFu, lo, src);
         best_hi = __shfl_sync(0xFFFFFFFFu, hi, src);
         have = true;
       }
-      next_off = min(next_off + 32, off_end);
+      next_off = min(next_off + 128, off_end);
     }
     // dynamic candidates below the stored one (a tie at its bit_offset sorts first)
     const uint64_t lim = have ? min(w1, best_lo + 1) : w1;
-    for (uint64_t p0 = w0; p0 < lim; p0 += 32) {
-      uint64_t p = p0 + lane;
-      bool hit = p < lim && dyn_candidate_fast(in, nbytes, p, leaf_lut);
-      uint32_t m = __ballot_sync(0xFFFFFFFFu, hit);
-      if (m) {
-        out_lo = out_hi = p0 + (__ffs(m) - 1);
-        return true;
+    const uint64_t pl = w0 + 32 * (uint64_t)lane;
+    uint32_t m = 0;
+    if (pl < lim) {
+      m = dyn_filter32(bits64_at(in32, pl));
+      if (pl + 32 > lim) m &= (1u << (lim - pl)) - 1;
+    }
+    int hit = -1;
+    while (m) {
+      const int i = __ffs(m) - 1;
+      m &= m - 1;
+      if (dyn_candidate_fast(in, nbytes, pl + i, leaf_lut)) {
+        hit = i;
+        break;
       }
+    }
+    const uint32_t b = __ballot_sync(0xFFFFFFFFu, hit >= 0);
+    if (b) {
+      const int src = __ffs(b) - 1;
+      const int i = __shfl_sync(0xFFFFFFFFu, hit, src);
+      out_lo = out_hi = w0 + 32 * (uint64_t)src + (uint64_t)i;
+      return true;
     }
     if (have && best_lo < w1) break;
   }

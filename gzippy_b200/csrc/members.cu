@@ -77,7 +77,15 @@ __global__ void stream_header_kernel(const uint8_t* __restrict__ in,
   info[s] = si;
 }
 
-// grid-stride over scan units (stream, byte range)
+// bit 7 of each byte of the result is set exactly where w's byte is zero
+__device__ __forceinline__ uint32_t zero_bytes(uint32_t w) {
+  const uint32_t t = (w & 0x7F7F7F7Fu) + 0x7F7F7F7Fu;
+  return ~(t | w | 0x7F7F7F7Fu);
+}
+
+// grid-stride over scan units (stream, byte range); each thread screens 16
+// aligned bytes at a time for the 0x1f of the magic with word operations
+// and tests only the positions that have one
 __global__ void member_scan_kernel(const uint8_t* __restrict__ in, const ScanUnit* __restrict__ units,
                                    uint32_t n_units, const uint64_t* __restrict__ s_off,
                                    const uint64_t* __restrict__ s_len,
@@ -89,26 +97,41 @@ __global__ void member_scan_kernel(const uint8_t* __restrict__ in, const ScanUni
     if (si.status != kOk) continue;
     const uint64_t base = s_off[su.stream], len = s_len[su.stream];
     const uint64_t lo = su.begin > (uint64_t)si.header_len + 1 ? su.begin : si.header_len + 1;
-    for (uint64_t pos = lo + threadIdx.x; pos < su.end; pos += blockDim.x) {
-      if (pos + 10 >= len || pos < 4) continue;
-      const uint8_t* q = in + base + pos;
-      if (q[0] != 0x1f || q[1] != 0x8b || q[2] != 8 || (q[3] & 0xE0)) continue;
-      uint32_t isz = q[-4] | (q[-3] << 8) | ((uint32_t)q[-2] << 16) | ((uint32_t)q[-1] << 24);
-      if (isz == 0 || isz > (1u << 30)) continue;
-      // header plausibility of is_likely_multi_member (format.rs:92-125):
-      // MTIME 0 or <= 4102444800, XFL in {0, 2, 4}, OS <= 13 or 255
-      uint32_t mtime = q[4] | (q[5] << 8) | ((uint32_t)q[6] << 16) | ((uint32_t)q[7] << 24);
-      if (mtime > 4102444800u) continue;
-      if (q[8] != 0 && q[8] != 2 && q[8] != 4) continue;
-      if (q[9] > 13 && q[9] != 255) continue;
-      uint32_t k = atomicAdd(n_cands, 1u);
-      if (k < cap) {
-        MemberCand c;
-        c.stream = su.stream;
-        c.pos = pos;
-        c.header_len = (uint32_t)parse_header(in, base + pos, base + len);
-        c.prev_isize = isz;
-        cands[k] = c;
+    for (uint64_t a = ((base + lo) & ~15ull) + 16 * (uint64_t)threadIdx.x; a < base + su.end;
+         a += 16 * (uint64_t)blockDim.x) {
+      const uint4 v = *reinterpret_cast<const uint4*>(in + a);
+      const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        uint32_t m = zero_bytes(w[k] ^ 0x1F1F1F1Fu);
+        while (m) {
+          const int j = (__ffs(m) - 1) >> 3;
+          m &= m - 1;
+          const uint64_t pos = a + 4 * k + j - base;
+          if (pos < lo || pos >= su.end) continue;
+          if (pos + 10 >= len || pos < 4) continue;
+          const uint8_t* q = in + base + pos;
+          if (q[0] != 0x1f || q[1] != 0x8b || q[2] != 8 || (q[3] & 0xE0)) continue;
+          const uint32_t isz =
+              q[-4] | (q[-3] << 8) | ((uint32_t)q[-2] << 16) | ((uint32_t)q[-1] << 24);
+          if (isz == 0 || isz > (1u << 30)) continue;
+          // header plausibility of is_likely_multi_member (format.rs:92-125):
+          // MTIME 0 or <= 4102444800, XFL in {0, 2, 4}, OS <= 13 or 255
+          const uint32_t mtime =
+              q[4] | (q[5] << 8) | ((uint32_t)q[6] << 16) | ((uint32_t)q[7] << 24);
+          if (mtime > 4102444800u) continue;
+          if (q[8] != 0 && q[8] != 2 && q[8] != 4) continue;
+          if (q[9] > 13 && q[9] != 255) continue;
+          const uint32_t kk = atomicAdd(n_cands, 1u);
+          if (kk < cap) {
+            MemberCand c;
+            c.stream = su.stream;
+            c.pos = pos;
+            c.header_len = (uint32_t)parse_header(in, base + pos, base + len);
+            c.prev_isize = isz;
+            cands[kk] = c;
+          }
+        }
       }
     }
   }
