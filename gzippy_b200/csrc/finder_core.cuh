@@ -171,6 +171,8 @@ static __device__ __noinline__ bool dyn_candidate_full(const uint8_t* in, uint64
         dist_gt1 += n_dist;
       }
       if (i <= 256 && 256 < i + rep) eob_len = v;
+      // Kraft sums only grow: an over-subscribed set fails the final test
+      if (lit_leaves > (1u << 15) || dist_leaves > (1u << 15)) return false;
     }
     prev = v;
     i += rep;
