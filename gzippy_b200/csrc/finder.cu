@@ -196,26 +196,39 @@ __global__ void __launch_bounds__(kSyncOffsets)
 // output byte per input byte (near-incompressible literals), 16 ms at 2.9
 // (text) and 29 ms at 13.6 (byte runs), and 0.6 ms for stored data.  So the
 // cost is the compressed bytes times (1 + 0.2 x the output-per-input estimate
-// of the dynamic header the chunk starts in), and a twentieth of that for a
-// stored start.
-__device__ float chunk_cost(const uint8_t* __restrict__ in, const ChunkDesc& d, uint64_t stop) {
-  const uint64_t nbits = d.in_end * 8;
-  uint64_t end = stop != kNoStop ? stop : nbits;
-  if (end > nbits) end = nbits;
-  const float span = end > d.start_bit ? (float)(end - d.start_bit) * 0.125f : 0.f;
+// of the dynamic header a chunk starts in), and a twentieth of that for a
+// stored start: the decode cost per compressed byte of the data a chunk
+// start begins in.
+__device__ float cost_factor(const uint8_t* __restrict__ in, const ChunkDesc& d) {
   float r = d.est_ratio;
   if (!(r > 0.f)) {
     // member starts and sync starts carry no finder estimate: take it from
     // the header of the block they start in
     const uint64_t hdr = (d.flags & kChunkSync) ? d.table_bit : d.start_bit;
     const uint32_t bt = hdr ? (uint32_t)(peek_bits(in, d.in_end, hdr, 3) >> 1) : 1u;
-    if (bt == 0) return 0.05f * span;
+    if (bt == 0) return 0.05f;
     if (bt == 2) r = dyn_header_ratio(in, d.in_end, hdr);
     if (!(r > 0.f)) r = 2.f;  // fixed-Huffman data: about 2 bytes per input byte
   } else if (r == 1.f && (peek_bits(in, d.in_end, d.start_bit, 3) >> 1) == 0) {
-    return 0.05f * span;  // a stored start
+    return 0.05f;  // a stored start
   }
-  return (1.f + 0.2f * r) * span;
+  return 1.f + 0.2f * r;
+}
+
+// A chunk's cost is its compressed bytes times the larger of the factors of
+// its own start and of its successor's, which shows the data at its far end:
+// a chunk that starts in stored data and runs into dense text or byte runs
+// is as costly as that data.
+__device__ float chunk_cost(const uint8_t* __restrict__ in, const ChunkDesc* descs,
+                            const ChunkDesc& d, uint64_t stop, uint32_t next) {
+  const uint64_t nbits = d.in_end * 8;
+  uint64_t end = stop != kNoStop ? stop : nbits;
+  if (end > nbits) end = nbits;
+  const float span = end > d.start_bit ? (float)(end - d.start_bit) * 0.125f : 0.f;
+  float f = cost_factor(in, d);
+  if (next != kNoChunk && !(descs[next].flags & kChunkMemberFirst))
+    f = fmaxf(f, cost_factor(in, descs[next]));
+  return f * span;
 }
 
 __global__ void link_kernel(const uint8_t* __restrict__ in, ChunkDesc* descs, uint32_t n,
@@ -252,7 +265,7 @@ __global__ void link_kernel(const uint8_t* __restrict__ in, ChunkDesc* descs, ui
   if ((d.flags & kChunkSync) && stop != kNoStop && stop > d.start_bit)
     s = min(slack, max(stop - d.start_bit, (uint64_t)kSyncMinSlack));
   d.abort_bit = (stop != kNoStop && !(d.flags & kChunkMemberFirst)) ? stop + s : kNoStop;
-  if (cost) cost[i] = chunk_cost(in, d, stop);
+  if (cost) cost[i] = chunk_cost(in, descs, d, stop, next);
   else work[atomicAdd(n_work, 1u)] = i;
 }
 
