@@ -18,7 +18,7 @@ namespace gzgpu {
 // the first candidate, split over the CTA's warps.  Stored candidates must
 // also pass start_ok (a stored or dynamic block right after them).
 constexpr int kFinderWarps = 8;
-constexpr uint64_t kFinderWindow = 1024;
+constexpr uint64_t kFinderWindow = 1024 * kFindGroup;  // bits a warp takes at a time
 
 // Stored block starts, searched first for every speculative chunk: the first
 // one (by byte offset, hence by start bit) in [guess_bit, limit_bit) whose
@@ -86,6 +86,7 @@ __global__ void __launch_bounds__(32 * kFinderWarps)
   __shared__ unsigned long long best_win;
   __shared__ uint64_t hit_lo[kFinderWarps], hit_hi[kFinderWarps], hit_win[kFinderWarps];
   __shared__ uint16_t leaf_lut[4096];
+  __shared__ FinderLists lists[kFinderWarps];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   if (blockIdx.x >= n_spec) return;
   ChunkDesc& d = descs[spec[blockIdx.x]];
@@ -102,7 +103,7 @@ __global__ void __launch_bounds__(32 * kFinderWarps)
     const uint64_t w1 = min(w0 + kFinderWindow, to);
     uint64_t lo = 0, hi = 0, s0 = w0;
     bool hit = false;
-    while (s0 < w1 && warp_find_first(in, nbytes, s0, w1, to, lane, lo, hi, leaf_lut)) {
+    while (s0 < w1 && warp_find_first(in, nbytes, s0, w1, to, lane, lo, hi, leaf_lut, &lists[warp])) {
       if (start_ok(in, nbytes, hi)) {
         hit = true;
         break;

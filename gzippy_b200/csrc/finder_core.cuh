@@ -181,12 +181,12 @@ static __device__ __noinline__ bool dyn_candidate_full(const uint8_t* in, uint64
   return kraft_exact(lit_leaves, lit_gt1) && kraft_exact(dist_leaves, dist_gt1);
 }
 
-// Full dynamic-header predicate at `bit` (13-bit header filter, precode leaf
-// count via `leaf_lut`, then dyn_candidate_full).  `leaf_lut` is the 4096-entry
-// leaf-count table, or null to count arithmetically.
-static __device__ __forceinline__ bool dyn_candidate_fast(const uint8_t* in, uint64_t nbytes,
-                                                          uint64_t bit,
-                                                          const uint16_t* leaf_lut) {
+// The cheap part of the dynamic-header predicate at `bit`: the 13-bit header
+// filter and the precode leaf count via `leaf_lut` (the 4096-entry leaf-count
+// table, or null to count arithmetically).  dyn_candidate_fast adds
+// dyn_candidate_full.
+static __device__ __forceinline__ bool dyn_leaf_ok(const uint8_t* in, uint64_t nbytes, uint64_t bit,
+                                                   const uint16_t* leaf_lut) {
   if (bit + 17 > nbytes * 8) return false;
   uint64_t x;
   uint32_t xh;
@@ -207,8 +207,13 @@ static __device__ __forceinline__ bool dyn_candidate_fast(const uint8_t* in, uin
              precode_leaves4((uint32_t)((pb >> 24) & 0xFFF)) +
              precode_leaves4((uint32_t)((pb >> 36) & 0xFFF)) + precode_leaves4((uint32_t)(pb >> 48));
   }
-  if (leaves != 128 && leaves != 64) return false;
-  return dyn_candidate_full(in, nbytes, bit);
+  return leaves == 128 || leaves == 64;
+}
+
+static __device__ __forceinline__ bool dyn_candidate_fast(const uint8_t* in, uint64_t nbytes,
+                                                          uint64_t bit,
+                                                          const uint16_t* leaf_lut) {
+  return dyn_leaf_ok(in, nbytes, bit, leaf_lut) && dyn_candidate_full(in, nbytes, bit);
 }
 
 // The block after a true non-final stored block starts at byte `n` (its
@@ -310,10 +315,133 @@ static __device__ __forceinline__ uint32_t stored_filter4(uint64_t B) {
 // and runs the full tests only on the offsets that pass (about 1 in 9 bits);
 // a ballot picks the lowest hit.  The first stored hit in byte order is the
 // smallest stored candidate, so the dynamic scan only needs to reach it.
+// Per-warp candidate lists of the grouped scan (finder kernel): positions of
+// one 1024-bit window that pass the 13-bit filter, then positions of a group
+// of windows that also pass the precode leaf count.
+constexpr uint32_t kFindGroup = 4;    // 1024-bit windows screened before the full tests
+constexpr uint32_t kFindFull = 64;    // leaf-count survivors held per group
+struct FinderLists {
+  uint16_t c1[1024];
+  uint32_t c2[kFindFull];
+  uint32_t n2;
+};
+
 static __device__ bool warp_find_first(const uint8_t* __restrict__ in, uint64_t nbytes,
                                        uint64_t from, uint64_t to, uint64_t hi_to, int lane,
                                        uint64_t& out_lo, uint64_t& out_hi,
-                                       const uint16_t* leaf_lut = nullptr) {
+                                       const uint16_t* leaf_lut = nullptr,
+                                       FinderLists* L = nullptr);
+
+// The same search with the dynamic tests spread over the warp: a group of
+// kFindGroup windows is screened (13-bit filter per lane, then the leaf
+// count for every survivor, 32 at a time), and the full tests of the group's
+// survivors run one per lane, the lowest passing position winning.  Used by
+// the finder kernel, whose warps have the lists in shared memory.
+static __device__ bool warp_find_first_grouped(const uint8_t* __restrict__ in, uint64_t nbytes,
+                                               uint64_t from, uint64_t to, uint64_t hi_to,
+                                               int lane, uint64_t& out_lo, uint64_t& out_hi,
+                                               const uint16_t* leaf_lut, FinderLists* L) {
+  const uint32_t* in32 = reinterpret_cast<const uint32_t*>(in);
+  if (to > nbytes * 8) to = nbytes * 8;
+  if (hi_to > nbytes * 8) hi_to = nbytes * 8;
+  bool have = false;
+  uint64_t best_lo = 0, best_hi = 0;
+  const uint64_t until = nbytes >= 5 ? min((hi_to + 7) / 8, nbytes - 4) : 0;
+  uint64_t next_off = max((from + 3 + 7) / 8, (uint64_t)2);
+  for (uint64_t g0 = from; g0 < to; g0 += 1024 * kFindGroup) {
+    const uint64_t g1 = min(g0 + 1024 * kFindGroup, to);
+    const uint64_t off_end = min(until, (g1 + 10) / 8 + 1);
+    while (!have && next_off < off_end) {
+      const uint64_t ob = next_off + 4 * (uint64_t)lane;
+      uint32_t m = 0;
+      if (ob < off_end) {
+        m = stored_filter4(bits64_at(in32, ob * 8));
+        if (ob + 4 > off_end) m &= (1u << (off_end - ob)) - 1;
+      }
+      uint64_t lo = 0, hi = 0;
+      bool hit = false;
+      while (m) {
+        const int k = __ffs(m) - 1;
+        m &= m - 1;
+        if (stored_candidate(in, nbytes, ob + k, from, to, hi_to, lo, hi)) {
+          hit = true;
+          break;
+        }
+      }
+      const uint32_t b = __ballot_sync(0xFFFFFFFFu, hit);
+      if (b) {
+        const int src = __ffs(b) - 1;
+        best_lo = __shfl_sync(0xFFFFFFFFu, lo, src);
+        best_hi = __shfl_sync(0xFFFFFFFFu, hi, src);
+        have = true;
+      }
+      next_off = min(next_off + 128, off_end);
+    }
+    const uint64_t lim = have ? min(g1, best_lo + 1) : g1;
+    if (lane == 0) L->n2 = 0;
+    __syncwarp();
+    for (uint64_t w0 = g0; w0 < lim; w0 += 1024) {
+      const uint64_t pl = w0 + 32 * (uint64_t)lane;
+      uint32_t m = 0;
+      if (pl < lim) {
+        m = dyn_filter32(bits64_at(in32, pl));
+        if (pl + 32 > lim) m &= (1u << (lim - pl)) - 1;
+      }
+      const uint32_t c = __popc(m);
+      uint32_t incl = c;
+#pragma unroll
+      for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t v = __shfl_up_sync(0xFFFFFFFFu, incl, d);
+        if (lane >= d) incl += v;
+      }
+      const uint32_t tot = __shfl_sync(0xFFFFFFFFu, incl, 31);
+      uint32_t k = incl - c;
+      while (m) {
+        const int i = __ffs(m) - 1;
+        m &= m - 1;
+        L->c1[k++] = (uint16_t)(32 * lane + i);
+      }
+      __syncwarp();
+      for (uint32_t j = lane; j < tot; j += 32) {
+        const uint64_t p = w0 + L->c1[j];
+        if (dyn_leaf_ok(in, nbytes, p, leaf_lut)) {
+          const uint32_t idx = atomicAdd(&L->n2, 1u);
+          if (idx < kFindFull) L->c2[idx] = (uint32_t)(p - g0);
+        }
+      }
+      __syncwarp();
+    }
+    const uint32_t n2 = L->n2;
+    if (n2 > kFindFull) {
+      // (rare: more survivors than the list holds) the lane-by-lane search
+      // from this group on gives the same answer
+      __syncwarp();
+      return warp_find_first(in, nbytes, g0, to, hi_to, lane, out_lo, out_hi, leaf_lut, nullptr);
+    }
+    uint64_t best = kNoStop;
+    for (uint32_t j = lane; j < n2; j += 32) {
+      const uint64_t p = g0 + L->c2[j];
+      if (p < best && dyn_candidate_full(in, nbytes, p)) best = p;
+    }
+#pragma unroll
+    for (int d = 16; d >= 1; d >>= 1) best = min(best, __shfl_xor_sync(0xFFFFFFFFu, best, d));
+    __syncwarp();
+    if (best != kNoStop) {
+      out_lo = out_hi = best;
+      return true;
+    }
+    if (have && best_lo < g1) break;
+  }
+  out_lo = best_lo;
+  out_hi = best_hi;
+  return have;
+}
+
+static __device__ bool warp_find_first(const uint8_t* __restrict__ in, uint64_t nbytes,
+                                       uint64_t from, uint64_t to, uint64_t hi_to, int lane,
+                                       uint64_t& out_lo, uint64_t& out_hi,
+                                       const uint16_t* leaf_lut, FinderLists* L) {
+  if (L) return warp_find_first_grouped(in, nbytes, from, to, hi_to, lane, out_lo, out_hi, leaf_lut, L);
   const uint32_t* in32 = reinterpret_cast<const uint32_t*>(in);
   if (to > nbytes * 8) to = nbytes * 8;
   if (hi_to > nbytes * 8) hi_to = nbytes * 8;
