@@ -103,7 +103,10 @@ __global__ void __launch_bounds__(32 * kFinderWarps)
     const uint64_t w1 = min(w0 + kFinderWindow, to);
     uint64_t lo = 0, hi = 0, s0 = w0;
     bool hit = false;
-    while (s0 < w1 && warp_find_first(in, nbytes, s0, w1, to, lane, lo, hi, leaf_lut, &lists[warp])) {
+    // stored candidates: the stored-start pass before this kernel took the
+    // first that could start this range, so only dynamic ones are left
+    while (s0 < w1 &&
+           warp_find_first(in, nbytes, s0, w1, to, lane, lo, hi, leaf_lut, &lists[warp], true)) {
       if (start_ok(in, nbytes, hi)) {
         hit = true;
         break;

@@ -330,17 +330,21 @@ static __device__ bool warp_find_first(const uint8_t* __restrict__ in, uint64_t 
                                        uint64_t from, uint64_t to, uint64_t hi_to, int lane,
                                        uint64_t& out_lo, uint64_t& out_hi,
                                        const uint16_t* leaf_lut = nullptr,
-                                       FinderLists* L = nullptr);
+                                       FinderLists* L = nullptr, bool dyn_only = false);
 
 // The same search with the dynamic tests spread over the warp: a group of
 // kFindGroup windows is screened (13-bit filter per lane, then the leaf
 // count for every survivor, 32 at a time), and the full tests of the group's
 // survivors run one per lane, the lowest passing position winning.  Used by
-// the finder kernel, whose warps have the lists in shared memory.
+// the finder kernel, whose warps have the lists in shared memory.  With
+// `dyn_only` the stored candidates are not searched (the finder kernel runs
+// after the stored-start pass, which took every stored candidate that could
+// start its range).
 static __device__ bool warp_find_first_grouped(const uint8_t* __restrict__ in, uint64_t nbytes,
                                                uint64_t from, uint64_t to, uint64_t hi_to,
                                                int lane, uint64_t& out_lo, uint64_t& out_hi,
-                                               const uint16_t* leaf_lut, FinderLists* L) {
+                                               const uint16_t* leaf_lut, FinderLists* L,
+                                               bool dyn_only) {
   const uint32_t* in32 = reinterpret_cast<const uint32_t*>(in);
   if (to > nbytes * 8) to = nbytes * 8;
   if (hi_to > nbytes * 8) hi_to = nbytes * 8;
@@ -351,7 +355,7 @@ static __device__ bool warp_find_first_grouped(const uint8_t* __restrict__ in, u
   for (uint64_t g0 = from; g0 < to; g0 += 1024 * kFindGroup) {
     const uint64_t g1 = min(g0 + 1024 * kFindGroup, to);
     const uint64_t off_end = min(until, (g1 + 10) / 8 + 1);
-    while (!have && next_off < off_end) {
+    while (!dyn_only && !have && next_off < off_end) {
       const uint64_t ob = next_off + 4 * (uint64_t)lane;
       uint32_t m = 0;
       if (ob < off_end) {
@@ -440,8 +444,10 @@ static __device__ bool warp_find_first_grouped(const uint8_t* __restrict__ in, u
 static __device__ bool warp_find_first(const uint8_t* __restrict__ in, uint64_t nbytes,
                                        uint64_t from, uint64_t to, uint64_t hi_to, int lane,
                                        uint64_t& out_lo, uint64_t& out_hi,
-                                       const uint16_t* leaf_lut, FinderLists* L) {
-  if (L) return warp_find_first_grouped(in, nbytes, from, to, hi_to, lane, out_lo, out_hi, leaf_lut, L);
+                                       const uint16_t* leaf_lut, FinderLists* L, bool dyn_only) {
+  if (L)
+    return warp_find_first_grouped(in, nbytes, from, to, hi_to, lane, out_lo, out_hi, leaf_lut, L,
+                                   dyn_only);
   const uint32_t* in32 = reinterpret_cast<const uint32_t*>(in);
   if (to > nbytes * 8) to = nbytes * 8;
   if (hi_to > nbytes * 8) hi_to = nbytes * 8;
