@@ -33,17 +33,83 @@ __device__ __forceinline__ const uint16_t* chunk_entry_page(const ChunkResult& r
   return pool.data + (size_t)page * kPageEntries;
 }
 
+// One warp writes the bytes of a span of 32 groups of 4 entries: lane L
+// holds the bytes of entries 4L .. 4L + 3 of the span in `w` (byte j of w =
+// entry 4L + j) and in `valid` which of them to write; `d0` is the output
+// address of the span's entry 0.  Each lane stores the aligned 32-bit word
+// that starts inside its group (its last bytes, then the next lane's first,
+// by a funnel shift), so a warp writes 128 contiguous bytes per store; bytes
+// of partly valid words and the two words the span shares with its
+// neighbours go out one by one.
+__device__ __forceinline__ void warp_store_bytes(uint8_t* __restrict__ out, uint64_t d0, uint32_t w,
+                                                 uint32_t valid, int lane) {
+  const uint32_t s = (uint32_t)(d0 & 3);
+  const uint64_t dl = d0 + 4 * (uint64_t)lane;
+  if (s == 0) {
+    if (valid == 0xFu) {
+      *reinterpret_cast<uint32_t*>(out + dl) = w;
+    } else {
+      for (int j = 0; j < 4; j++)
+        if ((valid >> j) & 1) out[dl + j] = (uint8_t)(w >> (8 * j));
+    }
+    return;
+  }
+  const uint32_t u = 4 - s;  // bytes of this group before the next aligned word
+  const uint32_t wn = __shfl_down_sync(0xFFFFFFFFu, w, 1);
+  const uint32_t vn = __shfl_down_sync(0xFFFFFFFFu, valid, 1);
+  if (lane < 31) {
+    const uint32_t vw = (valid >> u) | ((vn << s) & 0xFu);
+    const uint32_t ww = __funnelshift_r(w, wn, 8 * u);
+    if (vw == 0xFu) {
+      *reinterpret_cast<uint32_t*>(out + dl + u) = ww;
+    } else {
+      for (int j = 0; j < 4; j++)
+        if ((vw >> j) & 1) out[dl + u + j] = (uint8_t)(ww >> (8 * j));
+    }
+  } else {
+    for (uint32_t j = u; j < 4; j++)
+      if ((valid >> j) & 1) out[dl + j] = (uint8_t)(w >> (8 * j));
+  }
+  if (lane == 0)
+    for (uint32_t j = 0; j < u; j++)
+      if ((valid >> j) & 1) out[dl + j] = (uint8_t)(w >> (8 * j));
+}
+
+// the 4 entries of a group (page-relative index e, a multiple of 4)
+__device__ __forceinline__ void load_group(const uint16_t* page, uint32_t e, uint32_t v[4]) {
+  const uint2 x = *reinterpret_cast<const uint2*>(page + e);
+  v[0] = x.x & 0xFFFFu;
+  v[1] = x.x >> 16;
+  v[2] = x.y & 0xFFFFu;
+  v[3] = x.y >> 16;
+}
+
+// one CTA per chunk: the bytes of its last 32 KiB (markers written as 0,
+// which tail_markers_kernel replaces)
 __global__ void tail_literals_kernel(const PlacedChunk* __restrict__ placed, uint32_t n,
                                      const ChunkResult* __restrict__ results, PagePool pool,
                                      uint8_t* __restrict__ out) {
-  uint32_t k = blockIdx.x;
+  const uint32_t k = blockIdx.x;
   if (k >= n) return;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   const PlacedChunk pc = placed[k];
   const ChunkResult r = results[pc.chunk];
-  uint64_t len = r.out_len, t0 = len > kWindow ? len - kWindow : 0;
-  for (uint64_t q = t0 + threadIdx.x; q < len; q += blockDim.x) {
-    uint16_t v = chunk_entry_page(r, q, pool)[q % kPageEntries];
-    if (v < 256) out[pc.out_off + q] = (uint8_t)v;
+  const uint64_t len = r.out_len, t0 = len > kWindow ? len - kWindow : 0;
+  const uint64_t g0 = t0 & ~3ull;  // groups start at multiples of 4 (never across a page)
+  for (uint64_t base = g0 + 128 * (uint64_t)warp; base < len; base += 128 * (uint64_t)nwarps) {
+    const uint64_t q = base + 4 * (uint64_t)lane;
+    uint32_t w = 0, valid = 0;
+    if (q < len) {
+      uint32_t v[4];
+      load_group(chunk_entry_page(r, q, pool), (uint32_t)(q % kPageEntries), v);
+#pragma unroll
+      for (int j = 0; j < 4; j++)
+        if (q + j >= t0 && q + j < len) {
+          valid |= 1u << j;
+          w |= (v[j] < 256 ? v[j] : 0u) << (8 * j);
+        }
+    }
+    warp_store_bytes(out, pc.out_off + base, w, valid, lane);
   }
 }
 
@@ -73,14 +139,16 @@ __global__ void tail_markers_kernel(const PlacedChunk* __restrict__ placed,
   }
 }
 
-// one CTA per page; 8 entries per thread per step
+// one CTA per page: the entries before the chunk's tail, markers gathered
+// from the final window; 4 entries per lane, aligned 32-bit stores
 __global__ void body_kernel(const PlacedChunk* __restrict__ placed,
                             const uint32_t* __restrict__ placed_of_chunk, uint32_t n_pages,
                             const ChunkResult* __restrict__ results, PagePool pool,
                             uint8_t* __restrict__ out) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   for (uint32_t p = blockIdx.x; p < n_pages; p += gridDim.x) {
-    uint32_t cid = pool.owner[p];
-    uint32_t k = placed_of_chunk[cid];
+    const uint32_t cid = pool.owner[p];
+    const uint32_t k = placed_of_chunk[cid];
     if (k == 0xFFFFFFFFu) continue;
     const uint32_t sw = pool.seq[p];
     if ((sw >> kGenShift) != results[cid].gen) continue;  // page of a failed attempt
@@ -89,29 +157,29 @@ __global__ void body_kernel(const PlacedChunk* __restrict__ placed,
     const uint64_t t0 = len > kWindow ? len - kWindow : 0;
     const uint64_t q0 = (uint64_t)(sw & kSeqMask) * kPageEntries;
     if (q0 >= t0) continue;
-    uint64_t qend = q0 + kPageEntries;
-    if (qend > t0) qend = t0;
+    const uint32_t n = (uint32_t)min((uint64_t)kPageEntries, t0 - q0);
     const uint16_t* src = pool.data + (size_t)p * kPageEntries;
     const int64_t wbase = (int64_t)pc.out_off - (int64_t)kWindow - (int64_t)kMarkerBase;
-    for (uint64_t q = q0 + 8 * threadIdx.x; q < qend; q += 8 * blockDim.x) {
-      uint4 v4 = *reinterpret_cast<const uint4*>(src + (q - q0));
-      uint16_t e[8] = {(uint16_t)v4.x, (uint16_t)(v4.x >> 16), (uint16_t)v4.y,
-                       (uint16_t)(v4.y >> 16), (uint16_t)v4.z, (uint16_t)(v4.z >> 16),
-                       (uint16_t)v4.w, (uint16_t)(v4.w >> 16)};
-      uint8_t* dst = out + pc.out_off + q;
+    const int64_t moff = (int64_t)pc.member_off;
+    for (uint32_t base = 128 * warp; base < n; base += 128 * nwarps) {
+      const uint32_t e = base + 4 * lane;
+      uint32_t w = 0, valid = 0;
+      if (e < n) {
+        uint32_t v[4];
+        load_group(src, e, v);
 #pragma unroll
-      for (int j = 0; j < 8; j++) {
-        if (q + j >= qend) break;
-        uint16_t v = e[j];
-        uint8_t b;
-        if (v < 256) {
-          b = (uint8_t)v;
-        } else {
-          int64_t s = wbase + v;
-          b = s >= (int64_t)pc.member_off ? out[s] : 0;
-        }
-        dst[j] = b;
+        for (int j = 0; j < 4; j++)
+          if (e + j < n) {
+            valid |= 1u << j;
+            uint32_t b = v[j];
+            if (b >= 256) {
+              const int64_t sidx = wbase + b;
+              b = sidx >= moff ? out[sidx] : 0u;
+            }
+            w |= b << (8 * j);
+          }
       }
+      warp_store_bytes(out, pc.out_off + q0 + base, w, valid, lane);
     }
   }
 }
