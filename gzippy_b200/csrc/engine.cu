@@ -191,7 +191,7 @@ struct gzgpu_ctx {
   bool crc_ready = false;
 
   DevBuf in, out, s_off, s_len, info, units, cands, counters, descs, results, spec, work, cost;
-  DevBuf pages, owner, seq, placed, placed_of, list, segs, cblocks, bcrcs, mblk, mtrail, mlen,
+  DevBuf pages, owner, seq, placed, placed_of, list, cblocks, bcrcs, mblk, mtrail, mlen,
       mcrc, mstatus;
   // seek-index builds: the decoder's block log, the checkpoint interval and
   // the serialized index of the last job (gzgpu_build_index)
@@ -205,7 +205,7 @@ struct gzgpu_ctx {
   std::vector<DevBuf*> all_bufs() {
     return {&in,     &out,   &s_off,   &s_len,  &info,   &units,   &cands,  &counters, &descs,
             &results, &spec, &work,    &pages,  &owner,  &seq,     &placed, &placed_of, &list,
-            &segs,   &cblocks, &bcrcs, &mblk,   &mtrail, &mlen,    &mcrc,   &mstatus, &blk_log,
+            &cblocks, &bcrcs, &mblk,   &mtrail, &mlen,    &mcrc,   &mstatus, &blk_log,
             &cost};
   }
   const uint8_t* cur_in = nullptr;  // input buffer of the running job
@@ -1071,14 +1071,13 @@ int gzgpu_ctx::run(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R) 
   const uint32_t n_all = (uint32_t)hd.size();
   std::vector<PlacedChunk> placed;
   std::vector<uint32_t> placed_of(n_all, 0xFFFFFFFFu);
-  std::vector<uint32_t> tlist, tseg{0};
+  std::vector<uint32_t> tlist;  // placed chunks whose tails hold markers
   std::vector<CrcBlock> cblk;
   std::vector<uint32_t> mblk{0};
   std::vector<uint64_t> mtrail, mlenv;
   std::vector<std::pair<uint32_t, uint32_t>> mem_owner;  // (stream, member)
   uint64_t out_total = 0;
   const uint64_t kCrcBlock = 64 << 10;
-  uint64_t last_marker_end = 0;
   for (uint32_t s = 0; s < ns; s++) {
     for (Walker& w : SW[s])
       if (R[s].status == kOk) R[s].status = w.status;
@@ -1095,16 +1094,7 @@ int gzgpu_ctx::run(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R) 
         placed.push_back(PlacedChunk{out_total + so, moff, cid, 0});
         const ChunkResult& r = hr[cid];
         uint64_t t0 = r.out_len > kWindow ? r.out_len - kWindow : 0;
-        if (r.marker_end > t0) {
-          // a tail's markers read the 32 KiB before the chunk; they depend on
-          // the previous marker tail only if its output reaches into that
-          // window, otherwise a new independent run starts here
-          const uint64_t off = out_total + so;
-          if (tlist.size() > tseg.back() && last_marker_end + kWindow <= off)
-            tseg.push_back((uint32_t)tlist.size());
-          tlist.push_back((uint32_t)placed.size() - 1);
-          last_marker_end = off + r.out_len;
-        }
+        if (r.marker_end > t0) tlist.push_back((uint32_t)placed.size() - 1);
         so += r.out_len;
       }
       for (uint64_t b = 0; mp.trailer != kNoTrailer && b < mp.out_len; b += kCrcBlock)
@@ -1115,7 +1105,6 @@ int gzgpu_ctx::run(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R) 
       mlenv.push_back(mp.out_len);
       mem_owner.push_back({s, 0});
     }
-    if (tseg.back() != tlist.size()) tseg.push_back((uint32_t)tlist.size());
     R[s].out_len = so;
     out_total += so;
   }
@@ -1135,7 +1124,6 @@ int gzgpu_ctx::run(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R) 
   if ((rc = check(cur_out ? cudaSuccess : out.ensure(out_total + 64))) ||
       (rc = check(this->placed.ensure(sizeof(PlacedChunk) * (placed.size() + 1)))) ||
       (rc = check(this->placed_of.ensure(4 * (n_all + 1)))) || (rc = check(list.ensure(4 * (tlist.size() + 1)))) ||
-      (rc = check(segs.ensure(4 * (tseg.size() + 1)))) ||
       (rc = check(cblocks.ensure(sizeof(CrcBlock) * (cblk.size() + 1)))) ||
       (rc = check(bcrcs.ensure(4 * (cblk.size() + 1)))) || (rc = check(this->mblk.ensure(4 * (mblk.size() + 1)))) ||
       (rc = check(this->mtrail.ensure(8 * (mtrail.size() + 1)))) || (rc = check(mlen.ensure(8 * (mlenv.size() + 1)))) ||
@@ -1147,7 +1135,6 @@ int gzgpu_ctx::run(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R) 
                     cudaMemcpyHostToDevice, st);
   if (n_all) cudaMemcpyAsync(this->placed_of.p, placed_of.data(), 4 * n_all, cudaMemcpyHostToDevice, st);
   if (!tlist.empty()) cudaMemcpyAsync(list.p, tlist.data(), 4 * tlist.size(), cudaMemcpyHostToDevice, st);
-  cudaMemcpyAsync(segs.p, tseg.data(), 4 * tseg.size(), cudaMemcpyHostToDevice, st);
   if (!cblk.empty())
     cudaMemcpyAsync(cblocks.p, cblk.data(), sizeof(CrcBlock) * cblk.size(), cudaMemcpyHostToDevice, st);
   cudaMemcpyAsync(this->mblk.p, mblk.data(), 4 * mblk.size(), cudaMemcpyHostToDevice, st);
@@ -1167,8 +1154,8 @@ int gzgpu_ctx::run(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R) 
   if ((rc = check(launch_tail_literals(this->placed.as<PlacedChunk>(), np, results.as<ChunkResult>(),
                                        pool, cur_out, st))) ||
       (rc = check(launch_tail_markers(this->placed.as<PlacedChunk>(), list.as<uint32_t>(),
-                                      segs.as<uint32_t>(), (uint32_t)tseg.size() - 1,
-                                      results.as<ChunkResult>(), pool, cur_out, st))) ||
+                                      (uint32_t)tlist.size(), results.as<ChunkResult>(), pool,
+                                      cur_out, sms, st))) ||
       (rc = check(launch_body(this->placed.as<PlacedChunk>(), this->placed_of.as<uint32_t>(),
                               n_pages_used, results.as<ChunkResult>(), pool, cur_out, sms,
                               st))))

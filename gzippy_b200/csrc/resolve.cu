@@ -113,29 +113,50 @@ __global__ void tail_literals_kernel(const PlacedChunk* __restrict__ placed, uin
   }
 }
 
-// one CTA per run of the ordered tail-marker list: a run holds chunks whose
-// windows reach into each other's tails; runs (and streams) are independent.
-// Inside a run, chunks are resolved strictly in order.
+// The markers of chunk tails.  A tail marker names a byte of the 32 KiB
+// before its chunk, which lies in the tails of earlier chunks of the member
+// (a chunk shorter than 32 KiB is all tail); that entry is a literal or
+// again a marker, naming a byte before its own chunk.  Each marker follows
+// its references through the chunks' entries until it reaches a literal (or
+// a position before the member: 0), so all tails resolve in parallel: one
+// CTA per chunk of the list (the chunks whose tails hold markers), placed
+// chunks in output order.
 __global__ void tail_markers_kernel(const PlacedChunk* __restrict__ placed,
-                                    const uint32_t* __restrict__ list,
-                                    const uint32_t* __restrict__ seg_begin, uint32_t n_seg,
+                                    const uint32_t* __restrict__ list, uint32_t n_list,
                                     const ChunkResult* __restrict__ results, PagePool pool,
-                                    uint8_t* out) {
-  uint32_t s = blockIdx.x;
-  if (s >= n_seg) return;
-  for (uint32_t i = seg_begin[s]; i < seg_begin[s + 1]; i++) {
-    const PlacedChunk pc = placed[list[i]];
+                                    uint8_t* __restrict__ out) {
+  for (uint32_t i = blockIdx.x; i < n_list; i += gridDim.x) {
+    const uint32_t k = list[i];
+    const PlacedChunk pc = placed[k];
     const ChunkResult r = results[pc.chunk];
-    uint64_t len = r.out_len, t0 = len > kWindow ? len - kWindow : 0;
-    uint64_t end = r.marker_end < len ? r.marker_end : len;
+    const uint64_t len = r.out_len, t0 = len > kWindow ? len - kWindow : 0;
+    const uint64_t end = r.marker_end < len ? r.marker_end : len;
+    const int64_t moff = (int64_t)pc.member_off;
     for (uint64_t q = t0 + threadIdx.x; q < end; q += blockDim.x) {
-      uint16_t v = chunk_entry_page(r, q, pool)[q % kPageEntries];
-      if (v >= kMarkerBase) {
-        int64_t src = (int64_t)pc.out_off - (int64_t)kWindow + (int64_t)(v - kMarkerBase);
-        out[pc.out_off + q] = src >= (int64_t)pc.member_off ? out[src] : 0;
+      uint32_t v = chunk_entry_page(r, q, pool)[q % kPageEntries];
+      if (v < kMarkerBase) continue;  // a literal: written by tail_literals_kernel
+      uint32_t j = k;
+      int64_t off = (int64_t)pc.out_off;
+      uint32_t b = 0;
+      for (;;) {
+        const int64_t src = off - (int64_t)kWindow + (int64_t)(v - kMarkerBase);
+        if (src < moff) break;  // before the member: the zero window
+        // the chunk that holds src: one of the few before chunk j
+        do {
+          j--;
+        } while ((int64_t)placed[j].out_off > src);
+        const PlacedChunk pj = placed[j];
+        const ChunkResult rj = results[pj.chunk];
+        const uint64_t qj = (uint64_t)(src - (int64_t)pj.out_off);
+        v = chunk_entry_page(rj, qj, pool)[qj % kPageEntries];
+        if (v < kMarkerBase) {
+          b = v;
+          break;
+        }
+        off = (int64_t)pj.out_off;  // a marker of chunk j: its window is before chunk j
       }
+      out[pc.out_off + q] = (uint8_t)b;
     }
-    __syncthreads();
   }
 }
 
@@ -348,13 +369,12 @@ cudaError_t launch_tail_literals(const PlacedChunk* placed, uint32_t n, const Ch
   return cudaGetLastError();
 }
 
-cudaError_t launch_tail_markers(const PlacedChunk* placed, const uint32_t* list,
-                                const uint32_t* seg_begin, uint32_t n_seg,
+cudaError_t launch_tail_markers(const PlacedChunk* placed, const uint32_t* list, uint32_t n_list,
                                 const ChunkResult* results, const PagePool& pool, uint8_t* out,
-                                cudaStream_t stream) {
-  if (!n_seg) return cudaSuccess;
-  tail_markers_kernel<<<n_seg, 1024, 0, stream>>>(placed, list, seg_begin, n_seg, results, pool,
-                                                   out);
+                                int sms, cudaStream_t stream) {
+  if (!n_list) return cudaSuccess;
+  const uint32_t grid = n_list < (uint32_t)(sms * 8) ? n_list : (uint32_t)(sms * 8);
+  tail_markers_kernel<<<grid, 256, 0, stream>>>(placed, list, n_list, results, pool, out);
   return cudaGetLastError();
 }
 

@@ -9,10 +9,9 @@ namespace gzgpu {
 cudaError_t resolve_init(cudaStream_t stream);
 cudaError_t launch_tail_literals(const PlacedChunk* placed, uint32_t n, const ChunkResult* results,
                                  const PagePool& pool, uint8_t* out, cudaStream_t stream);
-cudaError_t launch_tail_markers(const PlacedChunk* placed, const uint32_t* list,
-                                const uint32_t* seg_begin, uint32_t n_seg,
+cudaError_t launch_tail_markers(const PlacedChunk* placed, const uint32_t* list, uint32_t n_list,
                                 const ChunkResult* results, const PagePool& pool, uint8_t* out,
-                                cudaStream_t stream);
+                                int sms, cudaStream_t stream);
 cudaError_t launch_body(const PlacedChunk* placed, const uint32_t* placed_of_chunk,
                         uint32_t n_pages, const ChunkResult* results, const PagePool& pool,
                         uint8_t* out, int sms, cudaStream_t stream);
