@@ -856,7 +856,7 @@ def main():
     clocks = clk.summary()
 
     # ---- e2e through the host C-ABI call with pinned buffers -------------------
-    e2e_steps = args.e2e_steps or max(1, min(args.steps, 3))
+    e2e_steps = args.e2e_steps or args.steps
     h_in = torch.from_numpy(comp).pin_memory()
     h_out = torch.empty(meta["plain_bytes"] + 4096, dtype=torch.uint8).pin_memory()
     hin_np, hout_np = h_in.numpy(), h_out.numpy()
@@ -874,9 +874,29 @@ def main():
     barrier()
     e2e_ms = max_over_ranks(f0.elapsed_time(f1), dist)
     e2e_ok = hashlib.sha256(hout_np[:n].tobytes()).hexdigest() == meta["sha256"]
+    # the same call with pageable buffers (a Rust Vec<u8> / numpy array that
+    # was never page-locked), as the drop-in shim passes them
+    p_in = np.array(comp, copy=True)
+    p_out = np.empty(meta["plain_bytes"] + 4096, np.uint8)
+    ctx.decompress_into(p_in, p_out)
+    barrier()
+    torch.cuda.synchronize()
+    g0 = torch.cuda.Event(enable_timing=True)
+    g1 = torch.cuda.Event(enable_timing=True)
+    g0.record()
+    for _ in range(e2e_steps):
+        ctx.decompress_into(p_in, p_out)
+    g1.record()
+    torch.cuda.synchronize()
+    barrier()
+    pg_ms = max_over_ranks(g0.elapsed_time(g1), dist)
+    pg_ok = hashlib.sha256(p_out[:n].tobytes()).hexdigest() == meta["sha256"]
     e2e = {"value": round(job_gbs(world, e2e_steps, meta["plain_bytes"], e2e_ms), 4),
            "unit": "GB/s", "h2d_bytes_per_step": int(comp.size),
-           "d2h_bytes_per_step": int(meta["plain_bytes"]), "byte_exact": bool(e2e_ok)}
+           "d2h_bytes_per_step": int(meta["plain_bytes"]), "byte_exact": bool(e2e_ok),
+           "host_buffers": "page-locked", "steps": e2e_steps,
+           "pageable": {"value": round(job_gbs(world, e2e_steps, meta["plain_bytes"], pg_ms), 4),
+                        "unit": "GB/s", "byte_exact": bool(pg_ok)}}
 
     # ---- roofline of the inflate kernel --------------------------------------
     peak, peak_kind = roofline_peak()
