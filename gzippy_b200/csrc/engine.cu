@@ -1359,12 +1359,6 @@ void gzgpu_destroy(gzgpu_ctx* c) {
 
 namespace {
 
-// host -> device copy of one stream into the context input buffer
-int stage_input(gzgpu_ctx* c, const uint8_t* in, size_t n, uint64_t at) {
-  cudaError_t e = cudaMemcpyAsync(c->in.as<uint8_t>() + at, in, n, cudaMemcpyHostToDevice, c->st);
-  return c->check(e);
-}
-
 void reset_stats(gzgpu_ctx* c) {
   c->stats = gzgpu_stats{};
   c->stats.lut_bits = c->lut_bits;
@@ -1377,6 +1371,123 @@ void finish_stats(gzgpu_ctx* c) {
   t = 0;
   cudaEventElapsedTime(&t, c->ev[0], c->ev[7]);
   c->stats.ms_total = t;
+}
+
+}  // namespace
+
+namespace {
+
+// Host copies: a stream in page-locked memory (in the batch path, one of at
+// least kDirectBytes) moves by DMA straight from / to the caller's buffer;
+// the others go through the context's pinned staging ring (stage.h: two
+// kStageSlot slots, allocated once), gathered and scattered by up to
+// kCopyThreads host threads while the other slot's DMA runs.
+constexpr size_t kDirectBytes = 1u << 20;
+constexpr int kCopyThreads = 8;
+
+bool host_pinned(const void* p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();  // pageable memory of an old driver reports an error: clear it
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+
+struct CopyJob {
+  void* dst;
+  const void* src;
+  size_t len;
+};
+
+void parallel_copy(const std::vector<CopyJob>& jobs) {
+  size_t total = 0;
+  for (const CopyJob& j : jobs) total += j.len;
+  int nt = (int)std::min<size_t>(kCopyThreads, total / (8u << 20) + 1);
+  nt = std::max(1, std::min(nt, (int)std::thread::hardware_concurrency()));
+  if (nt <= 1) {
+    for (const CopyJob& j : jobs) memcpy(j.dst, j.src, j.len);
+    return;
+  }
+  // split the byte range evenly; a job may be cut between threads
+  const size_t per = (total + nt - 1) / nt;
+  std::vector<std::thread> th;
+  for (int t = 0; t < nt; t++) {
+    th.emplace_back([&, t] {
+      const size_t b0 = t * per, b1 = std::min(total, b0 + per);
+      size_t at = 0;
+      for (const CopyJob& j : jobs) {
+        const size_t j0 = at, j1 = at + j.len;
+        at = j1;
+        if (j1 <= b0 || j0 >= b1) continue;
+        const size_t s0 = std::max(j0, b0) - j0, s1 = std::min(j1, b1) - j0;
+        memcpy((uint8_t*)j.dst + s0, (const uint8_t*)j.src + s0, s1 - s0);
+      }
+    });
+  }
+  for (std::thread& x : th) x.join();
+}
+
+// the staging ring's device side: copies and slot events on the context stream
+struct CudaStageOps {
+  gzgpu_ctx* c;
+  uint8_t* dev;  // device base of the staged byte offsets
+  int to_dev(uint64_t d, const uint8_t* src, uint64_t len) {
+    return c->check(cudaMemcpyAsync(dev + d, src, len, cudaMemcpyHostToDevice, c->st));
+  }
+  int to_host(uint8_t* dst, uint64_t d, uint64_t len) {
+    return c->check(cudaMemcpyAsync(dst, dev + d, len, cudaMemcpyDeviceToHost, c->st));
+  }
+  int record(int sl) { return c->check(cudaEventRecord(c->stage_ev[sl], c->st)); }
+  int wait(int sl) { return c->check(cudaEventSynchronize(c->stage_ev[sl])); }
+  void gather(const std::vector<StageHost>& h, uint8_t* slot) {
+    std::vector<CopyJob> jobs;
+    for (const StageHost& x : h) jobs.push_back(CopyJob{slot + x.slot_off, x.host, x.len});
+    parallel_copy(jobs);
+  }
+  void scatter(const std::vector<StageHost>& h, const uint8_t* slot) {
+    std::vector<CopyJob> jobs;
+    for (const StageHost& x : h) jobs.push_back(CopyJob{x.host, slot + x.slot_off, x.len});
+    parallel_copy(jobs);
+  }
+};
+
+// run the ring over `fills` (upload: host -> dev, else dev -> host); on
+// failure wait for the stream, so that no copy into or out of the ring
+// outlives the call
+int staged(gzgpu_ctx* c, const std::vector<StageFill>& fills, uint8_t* dev, bool upload) {
+  if (!c->h_stage.ensure(2 * kStageSlot)) return GZGPU_DEVICE_ERROR;
+  uint8_t* hb = reinterpret_cast<uint8_t*>(c->h_stage.p);
+  uint8_t* const slots[2] = {hb, hb + kStageSlot};
+  CudaStageOps ops{c, dev};
+  const int rc = upload ? stage_upload(fills, slots, ops) : stage_download(fills, slots, ops);
+  if (rc) cudaStreamSynchronize(c->st);
+  return rc;
+}
+
+// host -> device copy of one stream into the context input buffer at `at`:
+// page-locked caller memory by one DMA, pageable memory through the ring
+int stage_input(gzgpu_ctx* c, const uint8_t* in, size_t n, uint64_t at) {
+  if (!n) return kOk;
+  if (host_pinned(in))
+    return c->check(cudaMemcpyAsync(c->in.as<uint8_t>() + at, in, n, cudaMemcpyHostToDevice, c->st));
+  const std::vector<StageSeg> segs{StageSeg{const_cast<uint8_t*>(in), at, n}};
+  const std::vector<StageRun> runs{StageRun{at, at + n, 0, 1}};
+  return staged(c, stage_plan(segs, runs), c->in.as<uint8_t>(), true);
+}
+
+// device -> host copy of `n` output bytes at `off`, the same way round; all
+// of `out` is written when it returns
+int deliver_output(gzgpu_ctx* c, uint8_t* out, uint64_t off, size_t n) {
+  if (!n) return kOk;
+  if (host_pinned(out)) {
+    const int rc = c->check(cudaMemcpyAsync(out, c->cur_out + off, n, cudaMemcpyDeviceToHost, c->st));
+    if (rc) cudaStreamSynchronize(c->st);
+    return rc;
+  }
+  const std::vector<StageSeg> segs{StageSeg{out, off, n}};
+  const std::vector<StageRun> runs{StageRun{off, off + n, 0, 1}};
+  return staged(c, stage_plan(segs, runs), c->cur_out, false);
 }
 
 }  // namespace
@@ -1405,10 +1516,7 @@ int decompress_host(gzgpu_ctx* c, const uint8_t* in, size_t in_len, uint8_t* out
   if (R[0].out_len > out_cap) return GZGPU_OUT_TOO_SMALL;
   cudaEvent_t t0 = c->ev[8], t1 = c->ev[9];
   cudaEventRecord(t0, c->st);
-  if (R[0].out_len &&
-      (rc = c->check(cudaMemcpyAsync(out, c->cur_out + R[0].out_off, R[0].out_len,
-                                     cudaMemcpyDeviceToHost, c->st))))
-    return rc;
+  if ((rc = deliver_output(c, out, R[0].out_off, R[0].out_len))) return rc;
   cudaEventRecord(t1, c->st);
   if ((rc = c->check(cudaStreamSynchronize(c->st)))) return rc;
   float t = 0;
@@ -1612,98 +1720,6 @@ int gzgpu_decompress_batch_device(gzgpu_ctx* c, const void* d_in, const uint64_t
   if (all == GZGPU_OK && total > out_cap) return GZGPU_OUT_TOO_SMALL;
   return all;
 }
-
-namespace {
-
-// Host copies of the batch path: a stream of at least kDirectBytes in
-// page-locked memory moves by DMA straight from / to the caller's buffer;
-// the others go through the context's pinned staging ring (stage.h: two
-// kStageSlot slots, allocated once), gathered and scattered by up to
-// kCopyThreads host threads while the other slot's DMA runs.
-constexpr size_t kDirectBytes = 1u << 20;
-constexpr int kCopyThreads = 8;
-
-bool host_pinned(const void* p) {
-  cudaPointerAttributes a;
-  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
-    cudaGetLastError();  // pageable memory of an old driver reports an error: clear it
-    return false;
-  }
-  return a.type == cudaMemoryTypeHost;
-}
-
-struct CopyJob {
-  void* dst;
-  const void* src;
-  size_t len;
-};
-
-void parallel_copy(const std::vector<CopyJob>& jobs) {
-  size_t total = 0;
-  for (const CopyJob& j : jobs) total += j.len;
-  int nt = (int)std::min<size_t>(kCopyThreads, total / (8u << 20) + 1);
-  nt = std::max(1, std::min(nt, (int)std::thread::hardware_concurrency()));
-  if (nt <= 1) {
-    for (const CopyJob& j : jobs) memcpy(j.dst, j.src, j.len);
-    return;
-  }
-  // split the byte range evenly; a job may be cut between threads
-  const size_t per = (total + nt - 1) / nt;
-  std::vector<std::thread> th;
-  for (int t = 0; t < nt; t++) {
-    th.emplace_back([&, t] {
-      const size_t b0 = t * per, b1 = std::min(total, b0 + per);
-      size_t at = 0;
-      for (const CopyJob& j : jobs) {
-        const size_t j0 = at, j1 = at + j.len;
-        at = j1;
-        if (j1 <= b0 || j0 >= b1) continue;
-        const size_t s0 = std::max(j0, b0) - j0, s1 = std::min(j1, b1) - j0;
-        memcpy((uint8_t*)j.dst + s0, (const uint8_t*)j.src + s0, s1 - s0);
-      }
-    });
-  }
-  for (std::thread& x : th) x.join();
-}
-
-// the staging ring's device side: copies and slot events on the context stream
-struct CudaStageOps {
-  gzgpu_ctx* c;
-  uint8_t* dev;  // device base of the staged byte offsets
-  int to_dev(uint64_t d, const uint8_t* src, uint64_t len) {
-    return c->check(cudaMemcpyAsync(dev + d, src, len, cudaMemcpyHostToDevice, c->st));
-  }
-  int to_host(uint8_t* dst, uint64_t d, uint64_t len) {
-    return c->check(cudaMemcpyAsync(dst, dev + d, len, cudaMemcpyDeviceToHost, c->st));
-  }
-  int record(int sl) { return c->check(cudaEventRecord(c->stage_ev[sl], c->st)); }
-  int wait(int sl) { return c->check(cudaEventSynchronize(c->stage_ev[sl])); }
-  void gather(const std::vector<StageHost>& h, uint8_t* slot) {
-    std::vector<CopyJob> jobs;
-    for (const StageHost& x : h) jobs.push_back(CopyJob{slot + x.slot_off, x.host, x.len});
-    parallel_copy(jobs);
-  }
-  void scatter(const std::vector<StageHost>& h, const uint8_t* slot) {
-    std::vector<CopyJob> jobs;
-    for (const StageHost& x : h) jobs.push_back(CopyJob{x.host, slot + x.slot_off, x.len});
-    parallel_copy(jobs);
-  }
-};
-
-// run the ring over `fills` (upload: host -> dev, else dev -> host); on
-// failure wait for the stream, so that no copy into or out of the ring
-// outlives the call
-int staged(gzgpu_ctx* c, const std::vector<StageFill>& fills, uint8_t* dev, bool upload) {
-  if (!c->h_stage.ensure(2 * kStageSlot)) return GZGPU_DEVICE_ERROR;
-  uint8_t* hb = reinterpret_cast<uint8_t*>(c->h_stage.p);
-  uint8_t* const slots[2] = {hb, hb + kStageSlot};
-  CudaStageOps ops{c, dev};
-  const int rc = upload ? stage_upload(fills, slots, ops) : stage_download(fills, slots, ops);
-  if (rc) cudaStreamSynchronize(c->st);
-  return rc;
-}
-
-}  // namespace
 
 int gzgpu_decompress_batch(gzgpu_ctx* c, const gzgpu_span* ins, size_t n, gzgpu_out* outs,
                            int* statuses) {
