@@ -187,7 +187,7 @@ def bench_batch(args, rank: int, world: int, local: int):
     import torch
     torch.cuda.set_device(local)
     import gzippy_b200 as G
-    ctx = G.Context(device=local, autotune=not args.no_autotune)
+    ctx = G.Context(device=local, autotune=not args.no_autotune, decoder=args.decoder)
     d_in = torch.from_numpy(packed).cuda()
     total = meta["plain_bytes"]
     d_out = torch.empty(total + 4096, dtype=torch.uint8, device="cuda")
@@ -222,7 +222,7 @@ def bench_batch(args, rank: int, world: int, local: int):
     clocks = clk.summary()
 
     # ---- plain path: one stream per call, same streams, same GPU -------------
-    pctx = G.Context(device=local)
+    pctx = G.Context(device=local, decoder=args.decoder)
     aoff = np.zeros(n, np.uint64)
     at = 0
     for i in range(n):
@@ -345,7 +345,7 @@ def bench_sharded(args, rank: int, world: int, local: int, name: str, packed, of
             packed[int(offs[i]):int(offs[i]) + int(lens[i])]
     sub_lens = np.asarray(lens, np.uint64)[mine]
     total = int(np.asarray(sizes, np.int64)[mine].sum())
-    ctx = G.Context(device=local)
+    ctx = G.Context(device=local, decoder=args.decoder)
     d_in = torch.from_numpy(sub).cuda()
     d_out = torch.empty(total + 4096, dtype=torch.uint8, device="cuda")
 
@@ -736,6 +736,8 @@ def main():
     ap.add_argument("--lut-bits", type=int, default=0)
     ap.add_argument("--ctas-per-sm", type=int, default=0)
     ap.add_argument("--e2e-steps", type=int, default=0)
+    ap.add_argument("--decoder", type=int, default=0,
+                    help="Huffman block decoder: 0 default, 1 lane-parallel steps, 2 serial")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--rate", type=float, default=0.0, help="serving: arrivals/s (0 = 60%% of capacity)")
@@ -811,7 +813,7 @@ def main():
     config.update(plain_bytes=meta["plain_bytes"], comp_bytes=meta["comp_bytes"],
                       encoder=meta.get("encoder", "zlib-serial"))
     ctx = G.Context(device=local, chunk_bytes=args.chunk_bytes, lut_bits=args.lut_bits,
-                    ctas_per_sm=args.ctas_per_sm)
+                    ctas_per_sm=args.ctas_per_sm, decoder=args.decoder)
 
     # device-resident buffers (torch only allocates device memory here)
     pad = 1024

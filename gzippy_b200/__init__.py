@@ -53,7 +53,7 @@ class Config(ctypes.Structure):
                 ("lut_bits", ctypes.c_int), ("autotune", ctypes.c_int),
                 ("ring_history", ctypes.c_int), ("ctas_per_sm", ctypes.c_int),
                 ("fine_split", ctypes.c_int), ("high_priority", ctypes.c_int),
-                ("work_order", ctypes.c_int)]
+                ("work_order", ctypes.c_int), ("decoder", ctypes.c_int)]
 
 
 class Span(ctypes.Structure):
@@ -174,10 +174,10 @@ class Context:
     def __init__(self, device: int = 0, chunk_bytes: int = 0, lut_bits: int = 0,
                  autotune: bool = False, ring_history: bool = False, ctas_per_sm: int = 0,
                  fine_split: bool = False, high_priority: bool = False,
-                 longest_first: bool = True):
+                 longest_first: bool = True, decoder: int = 0):
         self._lib = lib()
         cfg = Config(device, chunk_bytes, lut_bits, int(autotune), int(ring_history), ctas_per_sm,
-                     int(fine_split), int(high_priority), 0 if longest_first else 1)
+                     int(fine_split), int(high_priority), 0 if longest_first else 1, decoder)
         h = ctypes.c_void_p()
         rc = self._lib.gzgpu_create(ctypes.byref(h), ctypes.byref(cfg))
         if rc != OK:

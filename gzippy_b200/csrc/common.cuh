@@ -123,6 +123,8 @@ struct PagePool {
   BlockRec* blocks = nullptr;
   uint32_t* n_blocks = nullptr;
   uint32_t blocks_cap = 0;
+  // Huffman block bodies: 0 = lane-parallel steps, 1 = warp-uniform serial
+  uint32_t serial = 0;
 };
 
 // resolve plan entry: one accepted chunk in output order

@@ -179,6 +179,7 @@ struct gzgpu_ctx {
   bool autotune = false;
   bool ring = false;  // history layout of the inflate kernel (false = pages)
   int ctas_per_sm = 3;  // page kernel CTAs per SM (3 or 4)
+  bool serial = false;  // warp-uniform serial block decode instead of lane-parallel steps
   bool fine_split = false;  // output-estimate pieces + dynamic-block sync starts
   bool high_priority = false;  // stream at the device's greatest priority
   bool lpt = true;             // decode work list longest-first (else in stream order)
@@ -225,6 +226,7 @@ struct gzgpu_ctx {
     PagePool pool{pages.as<uint16_t>(), owner.as<uint32_t>(), seq.as<uint32_t>(),
                   counters.as<uint32_t>() + 2, (uint32_t)(pages.cap / (kPageEntries * 2))};
     pool.cap = (uint32_t)std::min<uint64_t>(pool.cap, std::min(owner.cap, seq.cap) / 4);
+    pool.serial = serial ? 1u : 0u;
     if (job_index) {
       pool.blocks = blk_log.as<BlockRec>();
       pool.n_blocks = counters.as<uint32_t>() + 8;
@@ -1315,6 +1317,7 @@ int gzgpu_create(gzgpu_ctx** out, const gzgpu_config* cfg) {
     c->fine_split = cfg->fine_split != 0;
     c->high_priority = cfg->high_priority != 0;
     c->lpt = cfg->work_order == 0;
+    if (cfg->decoder == 1 || cfg->decoder == 2) c->serial = cfg->decoder == 2;
   }
   if (cudaSetDevice(c->dev) != cudaSuccess) {
     delete c;

@@ -535,13 +535,15 @@ __device__ __forceinline__ uint16_t* page_addr(const PageHist& ph, int32_t rel) 
 // kSync: the successor checks for sync starts and for starts gone by
 // mid-block (compiled out when the job has no sync starts)
 template <int LB, bool kSync>
-__device__ int32_t huff_block_parallel(BitReader& br, const Tables<LB>* T, PageHist& ph,
-                                       const PagePool& pool, uint32_t cid, uint32_t gen,
-                                       uint64_t& o, uint64_t& guard, uint64_t& marker_end,
-                                       bool zero_window, uint64_t trunc_words,
-                                       uint64_t sync_target, uint64_t passed_bit, bool& synced,
-                                       bool& passed, int lane) {
+__device__ __forceinline__ int32_t huff_block_parallel(
+    BitReader& br, const Tables<LB>* T, PageHist& ph_io, const PagePool& pool, uint32_t cid,
+    uint32_t gen, uint64_t& o_io, uint64_t& guard_io, uint64_t& marker_end_io, bool zero_window,
+    uint64_t trunc_words, uint64_t sync_target, uint64_t passed_bit, bool& synced, bool& passed,
+    int lane) {
   constexpr uint32_t LMASK = (1u << LB) - 1, DMASK = (1u << kDistBits) - 1;
+  // the loop state in registers, written back on return
+  PageHist ph = ph_io;
+  uint64_t o = o_io, guard = guard_io, marker_end = marker_end_io;
   uint64_t pos = br.pos();
   int32_t status = kOk;
   for (;;) {
@@ -746,7 +748,216 @@ __device__ int32_t huff_block_parallel(BitReader& br, const Tables<LB>* T, PageH
   }
   br.seek(pos, lane);
   br.refill(lane);
+  ph_io = ph;
+  o_io = o;
+  guard_io = guard;
+  marker_end_io = marker_end;
   return status;
+}
+
+// ---------------------------------------------------------------------------
+// Huffman block body, warp-uniform serial decode (page history).
+//
+// Every lane decodes the same symbol from the same bit window (table reads
+// are shared-memory broadcasts), so a literal costs one table lookup and a
+// few uniform ALU operations instead of 32 candidate decodes and a chain
+// walk.  Output entries gather in lane registers: lane k holds entry wb + k
+// of the current 32-entry aligned window (`cur`) and of the one before it
+// (`prv`); a full window goes to the pages as one coalesced 64-byte store.
+// A match fills the window lane-parallel: a source in `cur` or `prv` comes by
+// shuffle, an older one from the pages, a source inside the entries being
+// written by pointer jumping (sources lie strictly below their targets).
+// ---------------------------------------------------------------------------
+template <int LB, bool kSync>
+__device__ __forceinline__ int32_t huff_block_serial(
+    BitReader& br, const Tables<LB>* T, PageHist& ph_io, const PagePool& pool, uint32_t cid,
+    uint32_t gen, uint64_t& o_io, uint64_t& guard_io, uint64_t& marker_end_io, bool zero_window,
+    uint64_t trunc_words, uint64_t sync_target, uint64_t passed_bit, bool& synced, bool& passed,
+    int lane) {
+  constexpr uint32_t LMASK = (1u << LB) - 1, DMASK = (1u << kDistBits) - 1;
+  int32_t status = kOk;
+  // the loop state in registers, written back on return
+  PageHist ph = ph_io;
+  uint64_t o = o_io, guard = guard_io, marker_end = marker_end_io;
+  auto done = [&](int32_t st) {
+    ph_io = ph;
+    o_io = o;
+    guard_io = guard;
+    marker_end_io = marker_end;
+    return st;
+  };
+  if (o >= guard) {
+    ph.advance(o);
+    if (!ph.ensure(pool, cid, gen, o + kStepMaxOut, lane)) return done(kPoolExhausted);
+    const uint64_t pe = (ph.s + 1) << 16;
+    guard = ph.next != kNoPage ? pe : pe - kStepMaxOut;
+  }
+  // bit window: bits [pos, pos + bc) of the stream in bb, bc >= 32 before
+  // each code; word wn is appended next
+  const uint64_t pos0 = br.pos();
+  uint64_t wn = pos0 >> 5;
+  uint64_t bb = br.word(wn, lane) >> (pos0 & 31);
+  int bc = 32 - (int)(pos0 & 31);
+  wn++;
+  // value of entry q < 0 (before the chunk): zero or its window marker
+  auto before = [&](int64_t q) -> uint32_t {
+    return zero_window ? 0u : (uint32_t)((int64_t)(kMarkerBase + kWindow) + q);
+  };
+  // the register windows, reloaded from the pages at block entry
+  uint64_t wb = o & ~31ull;
+  uint32_t cur = 0, prv = 0;
+  {
+    __syncwarp();
+    if ((uint64_t)lane < o - wb) cur = *ph.at(wb + lane);
+    const int64_t q = (int64_t)wb - 32 + lane;
+    prv = q >= 0 ? (uint32_t)*ph.at((uint64_t)q) : before(q);
+  }
+  for (;;) {
+    if (o >= guard) {
+      ph.advance(o);
+      if (!ph.ensure(pool, cid, gen, o + kStepMaxOut, lane)) {
+        status = kPoolExhausted;
+        break;
+      }
+      const uint64_t pe = (ph.s + 1) << 16;
+      guard = ph.next != kNoPage ? pe : pe - kStepMaxOut;
+    }
+    if (kSync && wn * 32 - (uint64_t)bc == sync_target) {
+      synced = true;
+      break;
+    }
+    if (bc < 32) {
+      if (wn + 3 > br.limit_words) {
+        status = wn + 3 > trunc_words ? kTruncated : kOvershoot;
+        break;
+      }
+      bb |= (uint64_t)br.word(wn, lane) << bc;
+      bc += 32;
+      wn++;
+    }
+    uint32_t e = T->lit_lut[bb & LMASK];
+    if ((e & 15) == 0) {
+      e = slow_decode<LB>(bb, T->lit_count, T->lit_first, T->lit_offs, T->lit_sorted, litlen_entry);
+      if (e == 0) {
+        status = kBadDeflate;
+        break;
+      }
+    }
+    const uint32_t L = e & 15, kind = (e >> 8) & 3;
+    if (kind == kKindLit) {
+      bb >>= L;
+      bc -= (int)L;
+      if ((uint64_t)lane == o - wb) cur = e >> 16;
+      o++;
+      if (o - wb == 32) {
+        *ph.at(wb + lane) = (uint16_t)cur;
+        prv = cur;
+        wb += 32;
+      }
+      if (kSync && passed_bit < wn * 32 - (uint64_t)bc) {
+        passed = true;
+        break;
+      }
+      continue;
+    }
+    if (kind == kKindEob) {
+      bb >>= L;
+      bc -= (int)L;
+      break;
+    }
+    if (kind == kKindBad) {
+      status = kBadDeflate;
+      break;
+    }
+    const uint32_t xb = (e >> 4) & 15;
+    const uint32_t len = (e >> 16) + ((uint32_t)(bb >> L) & ((1u << xb) - 1));
+    bb >>= L + xb;
+    bc -= (int)(L + xb);
+    if (bc < 32) {
+      if (wn + 3 > br.limit_words) {
+        status = wn + 3 > trunc_words ? kTruncated : kOvershoot;
+        break;
+      }
+      bb |= (uint64_t)br.word(wn, lane) << bc;
+      bc += 32;
+      wn++;
+    }
+    uint32_t de = T->dist_lut[bb & DMASK];
+    if ((de & 15) == 0) {
+      de = slow_decode<kDistBits>(bb, T->dist_count, T->dist_first, T->dist_offs, T->dist_sorted,
+                                  dist_entry);
+      if (de == 0) {
+        status = kBadDeflate;
+        break;
+      }
+    }
+    if (((de >> 8) & 3) == kKindBad) {
+      status = kBadDeflate;
+      break;
+    }
+    const uint32_t DL = de & 15, dxb = (de >> 4) & 15;
+    const uint32_t dist = (de >> 16) + ((uint32_t)(bb >> DL) & ((1u << dxb) - 1));
+    bb >>= DL + dxb;
+    bc -= (int)(DL + dxb);
+    if ((uint64_t)dist > o + kWindow) {
+      status = kBadDeflate;
+      break;
+    }
+    // LZ77 copy: entry o + j = entry o + j - dist, window by window
+    for (uint32_t j0 = 0; j0 < len;) {
+      const uint32_t k0 = (uint32_t)(o - wb);  // first free lane of the window
+      const uint32_t n = min(32u - k0, len - j0);
+      const bool act = (uint32_t)lane >= k0 && (uint32_t)lane < k0 + n;
+      const int64_t src = (int64_t)wb + lane - (int64_t)dist;  // source of entry wb + lane
+      uint32_t v = 0;
+      int32_t ref = -1;  // a source among this pass's own entries: its lane
+      const int64_t rel = src - (int64_t)wb;
+      // an old source: from the pages (or before the chunk)
+      const bool old = act && rel < -32;
+      if (__any_sync(0xFFFFFFFFu, old)) {
+        __syncwarp();
+        if (old) v = src >= 0 ? (uint32_t)*ph.at((uint64_t)src) : before(src);
+      }
+      const uint32_t vc = __shfl_sync(0xFFFFFFFFu, cur, (int)(rel & 31));
+      const uint32_t vp = __shfl_sync(0xFFFFFFFFu, prv, (int)(rel & 31));
+      if (act && rel >= -32) {
+        if (rel < 0) v = vp;
+        else if (rel < (int64_t)k0) v = vc;
+        else ref = (int32_t)rel;
+      }
+      while (__any_sync(0xFFFFFFFFu, ref >= 0)) {
+        const uint32_t rv = __shfl_sync(0xFFFFFFFFu, v, ref & 31);
+        const int32_t rr = __shfl_sync(0xFFFFFFFFu, ref, ref & 31);
+        if (ref >= 0) {
+          v = rv;
+          ref = rr;
+        }
+      }
+      if (act) cur = v;
+      if (!zero_window) {
+        const uint32_t m = __ballot_sync(0xFFFFFFFFu, act && v >= kMarkerBase);
+        if (m) marker_end = wb + 32 - __clz(m);
+      }
+      o += n;
+      j0 += n;
+      if (o - wb == 32) {
+        *ph.at(wb + lane) = (uint16_t)cur;
+        prv = cur;
+        wb += 32;
+        __syncwarp();
+      }
+    }
+    if (kSync && passed_bit < wn * 32 - (uint64_t)bc) {
+      passed = true;
+      break;
+    }
+  }
+  // the open window's entries to the pages
+  if ((uint64_t)lane < o - wb) *ph.at(wb + lane) = (uint16_t)cur;
+  __syncwarp();
+  br.seek(wn * 32 - (uint64_t)bc, lane);
+  br.refill(lane);
+  return done(status);
 }
 
 // ---------------------------------------------------------------------------
@@ -990,9 +1201,14 @@ __device__ int32_t decode_chunk(const uint8_t* __restrict__ in, ChunkDesc d,
             passed_bit = ((const volatile ChunkDesc*)(descs + d.next))->start_bit;
         }
         bool passed = false;
-        status = huff_block_parallel<LB, kSync>(br, T, ph, pool, cid, gen, o, guard, marker_end,
-                                         zero_window, trunc_words, sync_target, passed_bit, synced,
-                                         passed, lane);
+        status = pool.serial
+                     ? huff_block_serial<LB, kSync>(br, T, ph, pool, cid, gen, o, guard, marker_end,
+                                                    zero_window, trunc_words, sync_target,
+                                                    passed_bit, synced, passed, lane)
+                     : huff_block_parallel<LB, kSync>(br, T, ph, pool, cid, gen, o, guard,
+                                                      marker_end, zero_window, trunc_words,
+                                                      sync_target, passed_bit, synced, passed,
+                                                      lane);
         if (status != kOk || synced) break;
         if (passed) {
           extend(descs[d.next].next);

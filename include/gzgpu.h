@@ -72,6 +72,9 @@ typedef struct {
                          contexts' streams (running blocks are not preempted) */
   int work_order;     /* order in which the persistent decoder takes chunks: 0 = longest
                          expected decode first (default), 1 = in stream order */
+  int decoder;        /* Huffman block bodies: 0 = default, 1 = lane-parallel steps (each
+                         lane decodes a candidate symbol at one bit offset), 2 = warp-uniform
+                         serial decode */
 } gzgpu_config;
 
 typedef struct {

@@ -22,11 +22,21 @@ def G():
     return G
 
 
-@pytest.fixture(scope="module")
-def ctx(G):
-    c = G.Context(chunk_bytes=32 << 10)
+# the two Huffman block decoders: lane-parallel steps and warp-uniform serial
+DECODERS = [1, 2]
+DECODER_IDS = ["steps", "serial"]
+
+
+@pytest.fixture(scope="module", params=DECODERS, ids=DECODER_IDS)
+def ctx(G, request):
+    c = G.Context(chunk_bytes=32 << 10, decoder=request.param)
     yield c
     c.close()
+
+
+# history layouts x decoders: (ring_history, decoder)
+LAYOUTS = [(False, 1), (False, 2), (True, 0)]
+LAYOUT_IDS = ["pages-steps", "pages-serial", "ring"]
 
 
 def _stream(ctype, level, n, seed=1):
@@ -72,10 +82,11 @@ def test_finder_matches_oracle(ctx):
             assert g == exp, (f, t, g, exp)
 
 
-@pytest.mark.parametrize("ring", [False, True], ids=["pages", "ring"])
-def test_decode_chunks_match_oracle(G, ring):
+@pytest.mark.parametrize("layout", LAYOUTS, ids=LAYOUT_IDS)
+def test_decode_chunks_match_oracle(G, layout):
     """Window-absent chunks from finder starts: entries, markers, end bits."""
-    ctx = G.Context(chunk_bytes=32 << 10, ring_history=ring)
+    ring, dec = layout
+    ctx = G.Context(chunk_bytes=32 << 10, ring_history=ring, decoder=dec)
     parts = [W.content(t, 5 + t, 1 << 20) for t in range(4)]
     plain = np.concatenate(parts)
     c = W.gzip_member(plain, 6)
@@ -104,15 +115,16 @@ def test_decode_chunks_match_oracle(G, ring):
 
 
 @pytest.mark.parametrize("encoder", ["zlib-serial", "pigz"])
-@pytest.mark.parametrize("ring", [False, True], ids=["pages", "ring"])
-def test_single_member_chunked_pipeline(G, ring, encoder):
+@pytest.mark.parametrize("layout", LAYOUTS, ids=LAYOUT_IDS)
+def test_single_member_chunked_pipeline(G, layout, encoder):
     """One member of mixed content, as one serial deflate stream and in the
     pigz-style framing (an empty stored block every MiB)."""
     parts = [W.content(t % 4, 100 + t, 1 << 20) for t in range(12)]
     plain = np.concatenate(parts)
     c = W.encode_member(plain, 6, encoder, threads=4)
+    ring, dec = layout
     for cb in (16 << 10, 64 << 10, 1 << 20):
-        ctx = G.Context(chunk_bytes=cb, ring_history=ring)
+        ctx = G.Context(chunk_bytes=cb, ring_history=ring, decoder=dec)
         got = ctx.decompress(c)
         s = ctx.stats()
         ctx.close()
