@@ -192,8 +192,8 @@ struct gzgpu_ctx {
   bool crc_ready = false;
 
   DevBuf in, out, s_off, s_len, info, units, cands, counters, descs, results, spec, work, cost;
-  DevBuf pages, owner, seq, placed, placed_of, list, cblocks, bcrcs, mblk, mtrail, mlen,
-      mcrc, mstatus;
+  DevBuf pages, owner, seq, placed, placed_of, list, cblocks, mend, mraw, mtrail, mlen, mcrc,
+      mstatus;
   // seek-index builds: the decoder's block log, the checkpoint interval and
   // the serialized index of the last job (gzgpu_build_index)
   DevBuf blk_log;
@@ -206,7 +206,7 @@ struct gzgpu_ctx {
   std::vector<DevBuf*> all_bufs() {
     return {&in,     &out,   &s_off,   &s_len,  &info,   &units,   &cands,  &counters, &descs,
             &results, &spec, &work,    &pages,  &owner,  &seq,     &placed, &placed_of, &list,
-            &cblocks, &bcrcs, &mblk,   &mtrail, &mlen,    &mcrc,   &mstatus, &blk_log,
+            &cblocks, &mend,  &mraw,   &mtrail, &mlen,    &mcrc,   &mstatus, &blk_log,
             &cost};
   }
   const uint8_t* cur_in = nullptr;  // input buffer of the running job
@@ -1075,11 +1075,8 @@ int gzgpu_ctx::run(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R) 
   std::vector<uint32_t> placed_of(n_all, 0xFFFFFFFFu);
   std::vector<uint32_t> tlist;  // placed chunks whose tails hold markers
   std::vector<CrcBlock> cblk;
-  std::vector<uint32_t> mblk{0};
-  std::vector<uint64_t> mtrail, mlenv;
-  std::vector<std::pair<uint32_t, uint32_t>> mem_owner;  // (stream, member)
+  std::vector<uint64_t> mtrail, mlenv, mendv;
   uint64_t out_total = 0;
-  const uint64_t kCrcBlock = 64 << 10;
   for (uint32_t s = 0; s < ns; s++) {
     for (Walker& w : SW[s])
       if (R[s].status == kOk) R[s].status = w.status;
@@ -1100,12 +1097,11 @@ int gzgpu_ctx::run(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R) 
         so += r.out_len;
       }
       for (uint64_t b = 0; mp.trailer != kNoTrailer && b < mp.out_len; b += kCrcBlock)
-        cblk.push_back(CrcBlock{moff + b, (uint32_t)std::min(kCrcBlock, mp.out_len - b),
+        cblk.push_back(CrcBlock{moff + b, (uint32_t)std::min<uint64_t>(kCrcBlock, mp.out_len - b),
                                 (uint32_t)mtrail.size()});
-      mblk.push_back((uint32_t)cblk.size());
       mtrail.push_back(mp.trailer);
       mlenv.push_back(mp.out_len);
-      mem_owner.push_back({s, 0});
+      mendv.push_back(moff + mp.out_len);
     }
     R[s].out_len = so;
     out_total += so;
@@ -1127,7 +1123,7 @@ int gzgpu_ctx::run(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R) 
       (rc = check(this->placed.ensure(sizeof(PlacedChunk) * (placed.size() + 1)))) ||
       (rc = check(this->placed_of.ensure(4 * (n_all + 1)))) || (rc = check(list.ensure(4 * (tlist.size() + 1)))) ||
       (rc = check(cblocks.ensure(sizeof(CrcBlock) * (cblk.size() + 1)))) ||
-      (rc = check(bcrcs.ensure(4 * (cblk.size() + 1)))) || (rc = check(this->mblk.ensure(4 * (mblk.size() + 1)))) ||
+      (rc = check(mend.ensure(8 * (mendv.size() + 1)))) || (rc = check(mraw.ensure(4 * (mtrail.size() + 1)))) ||
       (rc = check(this->mtrail.ensure(8 * (mtrail.size() + 1)))) || (rc = check(mlen.ensure(8 * (mlenv.size() + 1)))) ||
       (rc = check(mcrc.ensure(4 * (mtrail.size() + 1)))) ||
       (rc = check(mstatus.ensure(4 * (mtrail.size() + 1)))))
@@ -1139,10 +1135,11 @@ int gzgpu_ctx::run(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R) 
   if (!tlist.empty()) cudaMemcpyAsync(list.p, tlist.data(), 4 * tlist.size(), cudaMemcpyHostToDevice, st);
   if (!cblk.empty())
     cudaMemcpyAsync(cblocks.p, cblk.data(), sizeof(CrcBlock) * cblk.size(), cudaMemcpyHostToDevice, st);
-  cudaMemcpyAsync(this->mblk.p, mblk.data(), 4 * mblk.size(), cudaMemcpyHostToDevice, st);
   if (!mtrail.empty()) {
     cudaMemcpyAsync(this->mtrail.p, mtrail.data(), 8 * mtrail.size(), cudaMemcpyHostToDevice, st);
     cudaMemcpyAsync(mlen.p, mlenv.data(), 8 * mlenv.size(), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(mend.p, mendv.data(), 8 * mendv.size(), cudaMemcpyHostToDevice, st);
+    cudaMemsetAsync(mraw.p, 0, 4 * mtrail.size(), st);
   }
   if (!cur_out) cur_out = out.as<uint8_t>();
   PagePool pool{pages.as<uint16_t>(), owner.as<uint32_t>(), seq.as<uint32_t>(),
@@ -1164,7 +1161,7 @@ int gzgpu_ctx::run(const std::vector<StreamSpec>& S, std::vector<StreamOut>& R) 
     return rc;
   cudaEventRecord(ev[11], st);
   if ((rc = check(launch_crc(cblocks.as<CrcBlock>(), (uint32_t)cblk.size(), cur_out,
-                             bcrcs.as<uint32_t>(), this->mblk.as<uint32_t>(),
+                             mend.as<uint64_t>(), mraw.as<uint32_t>(),
                              this->mtrail.as<uint64_t>(), mlen.as<uint64_t>(),
                              (uint32_t)mtrail.size(), cur_in, mcrc.as<uint32_t>(),
                              mstatus.as<int32_t>(), sms, st))))

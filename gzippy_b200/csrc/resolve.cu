@@ -14,9 +14,11 @@
 //   body          : all other entries, fully parallel over pages, reading
 //                   windows the chain made final (resolve_and_narrow_markers
 //                   _in_place_crc, chunk_data.rs:1745)
-//   crc_blocks    : CRC32 of fixed-size blocks of output, lane-split
-//   crc_members   : GF(2) combine of block CRCs per member (crc32.rs
-//                   combine_crc32 :127), compared with the member trailer
+//   crc_blocks    : CRC32 of blocks of final output (up to 32 KiB of one
+//                   member each), each block's CRC moved to its member's end
+//                   and XORed into the member's register (crc32.rs
+//                   combine_crc32 :127 combines the same quantities)
+//   member_check  : each member's CRC32 and ISIZE against its trailer
 #include <cstdint>
 
 #include "common.cuh"
@@ -206,11 +208,20 @@ __global__ void body_kernel(const PlacedChunk* __restrict__ placed,
 }
 
 // ---------------------------------------------------------------------------
-// CRC32 (reflected 0xEDB88320): slice-by-8 tables in shared memory, GF(2)
-// combine crc(A|B) = x^(8|B|) * crc(A) + crc(B) mod P.
+// CRC32 (reflected 0xEDB88320).  A CRC register s followed by n zero bytes
+// becomes A^n(s) = s * x^(8n) mod P (linear in s), so
+//   raw(M1 | M2) = A^|M2|(raw(M1)) ^ raw(M2)       (raw: register starts at 0)
+//   crc(M)       = ~(A^|M|(0xFFFFFFFF) ^ raw(M))
+// and leading zero bytes leave raw() unchanged (crc32.rs combine_crc32 :127
+// combines the same quantities).  Each block's raw CRC is moved to its
+// member's end with A^(bytes after the block) and XORed into the member's
+// register, so blocks fold in independently, in any order.
 // ---------------------------------------------------------------------------
-__device__ uint32_t d_crc_tab[8][256];
-__device__ uint32_t d_x2n[64];  // x^(2^k) mod P
+__device__ uint32_t d_crc_tab[4][256];  // slice-by-4 tables
+__device__ uint32_t d_x2n[64];          // x^(2^k) mod P
+// d_crc_shift[j][k][v] = A^(kCrcSlice << j)(v << 8k): moves a register past
+// 2^j lane slices of zero bytes with 4 lookups
+__device__ uint32_t d_crc_shift[kCrcLevels][4][256];
 
 __device__ __forceinline__ uint32_t gf2_mulmod(uint32_t a, uint32_t b) {
   uint32_t r = 0;
@@ -227,12 +238,20 @@ __device__ __forceinline__ uint32_t x_pow_8n(uint64_t n) {
   uint32_t p = 1u << 31;
   uint64_t e = n << 3;
   for (int k = 0; e; e >>= 1, k++)
-    if (e & 1) p = gf2_mulmod(d_x2n[k & 31], p);
+    if (e & 1) p = gf2_mulmod(d_x2n[k & 63], p);
   return p;
 }
 
-__device__ __forceinline__ uint32_t crc_combine(uint32_t c1, uint32_t c2, uint64_t len2) {
-  return gf2_mulmod(x_pow_8n(len2), c1) ^ c2;
+// x^(8n) mod P computed by a whole warp: lane k takes exponent bits k and
+// k + 32, then a product tree over the lanes (every lane gets the result)
+__device__ __forceinline__ uint32_t x_pow_8n_warp(uint64_t n, int lane) {
+  const uint64_t e = n << 3;
+  uint32_t f = 1u << 31;
+  if ((e >> lane) & 1) f = d_x2n[lane];
+  if ((e >> (lane + 32)) & 1) f = gf2_mulmod(f, d_x2n[lane + 32]);
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) f = gf2_mulmod(f, __shfl_xor_sync(0xFFFFFFFFu, f, d));
+  return f;
 }
 
 __global__ void crc_init_kernel() {
@@ -241,7 +260,7 @@ __global__ void crc_init_kernel() {
   for (int k = 0; k < 8; k++) c = (c >> 1) ^ (0xEDB88320u & (0u - (c & 1u)));
   d_crc_tab[0][i] = c;
   __syncthreads();
-  for (int t = 1; t < 8; t++) {
+  for (int t = 1; t < 4; t++) {
     uint32_t p = d_crc_tab[t - 1][i];
     d_crc_tab[t][i] = (p >> 8) ^ d_crc_tab[0][p & 0xFF];
     __syncthreads();
@@ -255,111 +274,122 @@ __global__ void crc_init_kernel() {
   }
 }
 
-// one warp per CRC block; lane l hashes bytes [l*len/32, (l+1)*len/32)
-__global__ void crc_blocks_kernel(const CrcBlock* __restrict__ blocks, uint32_t n,
-                                  const uint8_t* __restrict__ out, uint32_t* __restrict__ crcs) {
-  __shared__ uint32_t tab[8][256];
-  for (int i = threadIdx.x; i < 8 * 256; i += blockDim.x) tab[i >> 8][i & 255] = d_crc_tab[i >> 8][i & 255];
+// one block per (level, byte slot): 256 register values each
+__global__ void crc_shift_init_kernel() {
+  const uint32_t j = blockIdx.x >> 2, k = blockIdx.x & 3, v = threadIdx.x;
+  const uint32_t xp = x_pow_8n((uint64_t)kCrcSlice << j);
+  d_crc_shift[j][k][v] = gf2_mulmod(xp, v << (8 * k));
+}
+
+// the register s moved past 2^j lane slices, from the shift tables in shared memory
+__device__ __forceinline__ uint32_t crc_shift(const uint32_t* shf, uint32_t s, int j) {
+  const uint32_t* t = shf + j * 1024;
+  return t[s & 0xFF] ^ t[256 + ((s >> 8) & 0xFF)] ^ t[512 + ((s >> 16) & 0xFF)] ^ t[768 + (s >> 24)];
+}
+
+// one byte into a CRC register, from the lane's own copy of the byte table
+// (word 32 * index + lane of the shared array: every lane of a warp reads
+// its own bank)
+__device__ __forceinline__ uint32_t crc_byte(const uint32_t* ltab, uint32_t lane, uint32_t c,
+                                             uint32_t b) {
+  return ltab[(((c ^ b) & 0xFFu) << 5) | lane] ^ (c >> 8);
+}
+
+// CRC32 of the final output, one warp per block of up to kCrcBlock bytes of
+// one member.  The block is cut into 32 lane slices of kCrcSlice bytes
+// counted back from its end, so every slice has the same length once the
+// bytes before the block count as zeros (they leave the register at 0).
+// Each lane folds its slice byte by byte with its own copy of the byte
+// table (no bank conflicts), reading aligned 16-byte words; the slices'
+// registers merge in a tree of fixed shifts, and the block's register,
+// moved past the rest of its member, is XORed into mem_raw.
+__global__ void __launch_bounds__(kCrcThreads)
+    crc_blocks_kernel(const CrcBlock* __restrict__ blocks, uint32_t n,
+                      const uint8_t* __restrict__ out, const uint64_t* __restrict__ mem_end,
+                      uint32_t* __restrict__ mem_raw) {
+  extern __shared__ __align__(16) uint32_t sm[];
+  uint32_t* ltab = sm;              // [256][32] lane copies of the byte table
+  uint32_t* shf = sm + 256 * 32;    // [kCrcLevels][4][256] shift tables
+  for (uint32_t i = threadIdx.x; i < 256 * 32; i += kCrcThreads) ltab[i] = d_crc_tab[0][i >> 5];
+  for (uint32_t i = threadIdx.x; i < kCrcLevels * 4 * 256; i += kCrcThreads)
+    shf[i] = d_crc_shift[i >> 10][(i >> 8) & 3][i & 255];
   __syncthreads();
   const int lane = threadIdx.x & 31;
-  for (uint32_t b = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; b < n;
-       b += (gridDim.x * blockDim.x) >> 5) {
-    const CrcBlock blk = blocks[b];
-    uint32_t per = (blk.len + 31) / 32;
-    per = (per + 7) & ~7u;
-    uint64_t s = (uint64_t)lane * per, e = s + per;
-    if (s > blk.len) s = blk.len;
-    if (e > blk.len) e = blk.len;
+  for (uint32_t bi = (blockIdx.x * kCrcThreads + threadIdx.x) >> 5; bi < n;
+       bi += (gridDim.x * kCrcThreads) >> 5) {
+    const CrcBlock blk = blocks[bi];
     const uint8_t* p = out + blk.off;
-    uint32_t c = 0xFFFFFFFFu;
-    uint64_t i = s;
-    // align to 8 bytes of the absolute address
-    while (i < e && ((blk.off + i) & 7)) c = (c >> 8) ^ tab[0][(c ^ p[i++]) & 0xFF];
-    for (; i + 8 <= e; i += 8) {
-      uint2 w = *reinterpret_cast<const uint2*>(p + i);
-      uint32_t lo = w.x ^ c, hi = w.y;
-      c = tab[7][lo & 0xFF] ^ tab[6][(lo >> 8) & 0xFF] ^ tab[5][(lo >> 16) & 0xFF] ^
-          tab[4][lo >> 24] ^ tab[3][hi & 0xFF] ^ tab[2][(hi >> 8) & 0xFF] ^
-          tab[1][(hi >> 16) & 0xFF] ^ tab[0][hi >> 24];
-    }
-    while (i < e) c = (c >> 8) ^ tab[0][(c ^ p[i++]) & 0xFF];
-    c = ~c;
-    uint64_t len = e - s;
-    // tree combine across lanes, left to right
+    const uint8_t* end = p + blk.len;
+    // lane slice [s0, s1), clipped to the block
+    const int64_t back = (int64_t)kCrcSlice * (32 - lane);
+    const uint8_t* s1 = end - (back - kCrcSlice);
+    const uint8_t* s0 = (int64_t)blk.len > back - kCrcSlice ? (back <= (int64_t)blk.len ? end - back : p) : s1;
+    uint32_t c = 0;
+    const uint8_t* q = s0;
+    // bytes up to the first 16-byte boundary
+    while (q < s1 && (reinterpret_cast<uintptr_t>(q) & 15)) c = crc_byte(ltab, lane, c, *q++);
+    // aligned 16-byte words, the next one loaded while this one folds
+    if (q + 16 <= s1) {
+      uint4 w = *reinterpret_cast<const uint4*>(q);
+      for (;;) {
+        const bool more = q + 32 <= s1;
+        uint4 nx = more ? *reinterpret_cast<const uint4*>(q + 16) : make_uint4(0, 0, 0, 0);
+        const uint32_t wd[4] = {w.x, w.y, w.z, w.w};
 #pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-      uint32_t c2 = __shfl_down_sync(0xFFFFFFFFu, c, d);
-      uint64_t l2 = __shfl_down_sync(0xFFFFFFFFu, len, d);
-      if ((lane & (2 * d - 1)) == 0 && lane + d < 32) {
-        c = crc_combine(c, c2, l2);
-        len += l2;
+        for (int k = 0; k < 4; k++) {
+          c = crc_byte(ltab, lane, c, wd[k]);
+          c = crc_byte(ltab, lane, c, wd[k] >> 8);
+          c = crc_byte(ltab, lane, c, wd[k] >> 16);
+          c = crc_byte(ltab, lane, c, wd[k] >> 24);
+        }
+        q += 16;
+        if (!more) break;
+        w = nx;
       }
     }
-    if (lane == 0) crcs[b] = c;
+    while (q < s1) c = crc_byte(ltab, lane, c, *q++);
+    // slices merge: 2^j slices on each side at level j
+#pragma unroll
+    for (int j = 0; j < 5; j++) {
+      const uint32_t r = __shfl_down_sync(0xFFFFFFFFu, c, 1 << j);
+      if ((lane & ((2 << j) - 1)) == 0) c = crc_shift(shf, c, j) ^ r;
+    }
+    // move the block's register past the rest of its member
+    const uint32_t xp = x_pow_8n_warp(mem_end[blk.member] - (blk.off + blk.len), lane);
+    if (lane == 0) atomicXor(mem_raw + blk.member, gf2_mulmod(xp, c));
   }
 }
 
-// one CTA per member: combine its block CRCs in order, check the trailer
-__global__ void crc_members_kernel(const CrcBlock* __restrict__ blocks,
-                                   const uint32_t* __restrict__ block_crcs,
-                                   const uint32_t* __restrict__ mem_block_begin,
-                                   const uint64_t* __restrict__ mem_trailer,
-                                   const uint64_t* __restrict__ mem_len, uint32_t n_mem,
-                                   const uint8_t* __restrict__ in, uint32_t* __restrict__ mem_crc,
-                                   int32_t* __restrict__ mem_status) {
-  __shared__ uint32_t sc[256];
-  __shared__ uint64_t sl[256];
-  uint32_t m = blockIdx.x;
+// one thread per member: its CRC from the accumulated blocks, checked with
+// the trailer's CRC32 and ISIZE
+__global__ void member_check_kernel(const uint64_t* __restrict__ mem_trailer,
+                                    const uint64_t* __restrict__ mem_len, uint32_t n_mem,
+                                    const uint8_t* __restrict__ in,
+                                    const uint32_t* __restrict__ mem_raw,
+                                    uint32_t* __restrict__ mem_crc, int32_t* __restrict__ mem_status) {
+  const uint32_t m = blockIdx.x * blockDim.x + threadIdx.x;
   if (m >= n_mem) return;
-  uint32_t b0 = mem_block_begin[m], b1 = mem_block_begin[m + 1];
-  uint32_t nb = b1 - b0;
-  // each thread folds a contiguous run of blocks
-  uint32_t per = (nb + blockDim.x - 1) / blockDim.x;
-  uint32_t s = threadIdx.x * per, e = min(s + per, nb);
-  uint32_t c = 0;
-  uint64_t len = 0;
-  for (uint32_t i = s; i < e; i++) {
-    c = len == 0 ? block_crcs[b0 + i] : crc_combine(c, block_crcs[b0 + i], blocks[b0 + i].len);
-    len += blocks[b0 + i].len;
+  const uint64_t t = mem_trailer[m];
+  int32_t st = kOk;
+  uint32_t crc = 0;
+  if (t != kNoTrailer) {
+    crc = ~(gf2_mulmod(x_pow_8n(mem_len[m]), 0xFFFFFFFFu) ^ mem_raw[m]);
+    const uint32_t ecrc = in[t] | (in[t + 1] << 8) | ((uint32_t)in[t + 2] << 16) | ((uint32_t)in[t + 3] << 24);
+    const uint32_t eisz = in[t + 4] | (in[t + 5] << 8) | ((uint32_t)in[t + 6] << 16) | ((uint32_t)in[t + 7] << 24);
+    if ((uint32_t)mem_len[m] != eisz) st = kSizeMismatch;
+    else if (crc != ecrc) st = kCrcMismatch;
   }
-  sc[threadIdx.x] = c;
-  sl[threadIdx.x] = len;
-  __syncthreads();
-  for (int d = 1; d < (int)blockDim.x; d <<= 1) {
-    uint32_t cc = 0;
-    uint64_t ll = 0;
-    bool act = (threadIdx.x & (2 * d - 1)) == 0 && threadIdx.x + d < blockDim.x;
-    if (act) {
-      uint32_t c2 = sc[threadIdx.x + d];
-      uint64_t l2 = sl[threadIdx.x + d];
-      cc = sl[threadIdx.x] == 0 ? c2 : (l2 == 0 ? sc[threadIdx.x] : crc_combine(sc[threadIdx.x], c2, l2));
-      ll = sl[threadIdx.x] + l2;
-    }
-    __syncthreads();
-    if (act) {
-      sc[threadIdx.x] = cc;
-      sl[threadIdx.x] = ll;
-    }
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) {
-    uint32_t crc = sc[0];
-    mem_crc[m] = crc;
-    uint64_t t = mem_trailer[m];
-    int32_t st = kOk;
-    if (t != kNoTrailer) {
-      uint32_t ecrc = in[t] | (in[t + 1] << 8) | ((uint32_t)in[t + 2] << 16) | ((uint32_t)in[t + 3] << 24);
-      uint32_t eisz = in[t + 4] | (in[t + 5] << 8) | ((uint32_t)in[t + 6] << 16) | ((uint32_t)in[t + 7] << 24);
-      if ((uint32_t)mem_len[m] != eisz) st = kSizeMismatch;
-      else if (crc != ecrc) st = kCrcMismatch;
-    }
-    mem_status[m] = st;
-  }
+  mem_crc[m] = crc;
+  mem_status[m] = st;
 }
 
 cudaError_t resolve_init(cudaStream_t stream) {
   crc_init_kernel<<<1, 256, 0, stream>>>();
-  return cudaGetLastError();
+  crc_shift_init_kernel<<<4 * kCrcLevels, 256, 0, stream>>>();
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(crc_blocks_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)kCrcSmem);
 }
 
 cudaError_t launch_tail_literals(const PlacedChunk* placed, uint32_t n, const ChunkResult* results,
@@ -388,20 +418,20 @@ cudaError_t launch_body(const PlacedChunk* placed, const uint32_t* placed_of_chu
 }
 
 cudaError_t launch_crc(const CrcBlock* blocks, uint32_t n_blocks, const uint8_t* out,
-                       uint32_t* block_crcs, const uint32_t* mem_block_begin,
-                       const uint64_t* mem_trailer, const uint64_t* mem_len, uint32_t n_mem,
-                       const uint8_t* in, uint32_t* mem_crc, int32_t* mem_status, int sms,
-                       cudaStream_t stream) {
+                       const uint64_t* mem_end, uint32_t* mem_raw, const uint64_t* mem_trailer,
+                       const uint64_t* mem_len, uint32_t n_mem, const uint8_t* in,
+                       uint32_t* mem_crc, int32_t* mem_status, int sms, cudaStream_t stream) {
   if (n_blocks) {
-    uint32_t warps = n_blocks;
-    uint32_t blocks_needed = (warps + 7) / 8;
-    uint32_t grid = blocks_needed < (uint32_t)(sms * 8) ? blocks_needed : (uint32_t)(sms * 8);
-    crc_blocks_kernel<<<grid, 256, 0, stream>>>(blocks, n_blocks, out, block_crcs);
+    const uint32_t warps_per_cta = kCrcThreads / 32;
+    const uint32_t need = (n_blocks + warps_per_cta - 1) / warps_per_cta;
+    const uint32_t cap = (uint32_t)sms * kCrcCtasPerSm;
+    const uint32_t grid = need < cap ? need : cap;
+    crc_blocks_kernel<<<grid, kCrcThreads, kCrcSmem, stream>>>(blocks, n_blocks, out, mem_end,
+                                                               mem_raw);
   }
-  if (n_mem) {
-    crc_members_kernel<<<n_mem, 256, 0, stream>>>(blocks, block_crcs, mem_block_begin, mem_trailer,
-                                                   mem_len, n_mem, in, mem_crc, mem_status);
-  }
+  if (n_mem)
+    member_check_kernel<<<(n_mem + 255) / 256, 256, 0, stream>>>(mem_trailer, mem_len, n_mem, in,
+                                                                  mem_raw, mem_crc, mem_status);
   return cudaGetLastError();
 }
 
