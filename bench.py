@@ -737,7 +737,7 @@ def main():
     ap.add_argument("--ctas-per-sm", type=int, default=0)
     ap.add_argument("--e2e-steps", type=int, default=0)
     ap.add_argument("--decoder", type=int, default=0,
-                    help="Huffman block decoder: 0 default, 1 lane-parallel steps, 2 serial")
+                    help="Huffman block decoder: 0 default, 1 lane-parallel 32-bit steps, 2 serial, 3 64-bit steps, 4 per block")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--rate", type=float, default=0.0, help="serving: arrivals/s (0 = 60%% of capacity)")

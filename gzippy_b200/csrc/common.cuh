@@ -123,7 +123,9 @@ struct PagePool {
   BlockRec* blocks = nullptr;
   uint32_t* n_blocks = nullptr;
   uint32_t blocks_cap = 0;
-  // Huffman block bodies: 0 = lane-parallel steps, 1 = warp-uniform serial
+  // Huffman block bodies: 0 = lane-parallel 32-bit steps, 1 = warp-uniform
+  // serial, 2 = lane-parallel 64-bit steps with matches decoded on the walk,
+  // 3 = per block, 2 for literal-heavy blocks and 0 for the others
   uint32_t serial = 0;
 };
 

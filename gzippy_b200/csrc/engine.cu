@@ -179,7 +179,7 @@ struct gzgpu_ctx {
   bool autotune = false;
   bool ring = false;  // history layout of the inflate kernel (false = pages)
   int ctas_per_sm = 3;  // page kernel CTAs per SM (3 or 4)
-  bool serial = false;  // warp-uniform serial block decode instead of lane-parallel steps
+  uint32_t decoder_mode = 3;  // PagePool::serial: Huffman block decoder (3: chosen per block)
   bool fine_split = false;  // output-estimate pieces + dynamic-block sync starts
   bool high_priority = false;  // stream at the device's greatest priority
   bool lpt = true;             // decode work list longest-first (else in stream order)
@@ -226,7 +226,7 @@ struct gzgpu_ctx {
     PagePool pool{pages.as<uint16_t>(), owner.as<uint32_t>(), seq.as<uint32_t>(),
                   counters.as<uint32_t>() + 2, (uint32_t)(pages.cap / (kPageEntries * 2))};
     pool.cap = (uint32_t)std::min<uint64_t>(pool.cap, std::min(owner.cap, seq.cap) / 4);
-    pool.serial = serial ? 1u : 0u;
+    pool.serial = decoder_mode;
     if (job_index) {
       pool.blocks = blk_log.as<BlockRec>();
       pool.n_blocks = counters.as<uint32_t>() + 8;
@@ -1314,7 +1314,10 @@ int gzgpu_create(gzgpu_ctx** out, const gzgpu_config* cfg) {
     c->fine_split = cfg->fine_split != 0;
     c->high_priority = cfg->high_priority != 0;
     c->lpt = cfg->work_order == 0;
-    if (cfg->decoder == 1 || cfg->decoder == 2) c->serial = cfg->decoder == 2;
+    // decoder 1: lane-parallel 32-bit steps, 2: serial, 3: 64-bit steps,
+    // 4: chosen per block
+    static const uint32_t kMode[5] = {0u, 0u, 1u, 2u, 3u};
+    if (cfg->decoder >= 1 && cfg->decoder <= 4) c->decoder_mode = kMode[cfg->decoder];
   }
   if (cudaSetDevice(c->dev) != cudaSuccess) {
     delete c;

@@ -72,21 +72,34 @@ __device__ __forceinline__ uint32_t dist_entry(uint32_t sym, uint32_t L) {
 }
 __device__ __forceinline__ uint32_t pre_entry(uint32_t sym, uint32_t L) { return (sym << 16) | L; }
 
+// 64-bit steps: entries of a step with matches staged in shared memory
+// (larger steps write their pages directly)
+constexpr uint32_t kWideStage = 256;
+
 // Per-warp Huffman tables (shared memory).
 template <int LB>
 struct alignas(16) Tables {
   uint32_t lit_lut[1 << LB];
   uint32_t dist_lut[1 << kDistBits];
-  uint32_t pre_lut[128];
   uint16_t lit_sorted[288];
   uint16_t dist_sorted[32];
-  uint16_t pre_sorted[20];
   uint16_t lit_count[16], lit_first[16], lit_offs[16];
   uint16_t dist_count[16], dist_first[16], dist_offs[16];
   uint16_t pre_count[16], pre_first[16], pre_offs[16];
   uint16_t next[16];
-  uint8_t lens[320];
+  union {
+    struct {  // a block header's code lengths (read_tables only)
+      uint32_t pre_lut[128];
+      uint16_t pre_sorted[20];
+      uint8_t lens[320];
+    };
+    struct {                       // 64-bit steps (huff_block_wide only)
+      uint16_t stage[kWideStage];  // the entries of a step with matches
+      uint8_t succ[64];            // a literal's successor bit per step bit (0xFF: other)
+    };
+  };
   uint8_t smap[32];  // output pass: lane of the symbol starting at each entry
+  float p_len;       // the block's code space taken by length codes (sum of 2^-length)
 };
 
 template <int LB>
@@ -281,6 +294,8 @@ __device__ int32_t read_tables(BitReader& br, uint32_t btype, Tables<LB>* T, uin
     ok = ok && build_table<kDistBits>(T->lens + 288, 32, T->dist_count, T->dist_first,
                                       T->dist_offs, T->dist_sorted, T->next, T->dist_lut, lane,
                                       dist_entry);
+    if (lane == 0) T->p_len = 24.f / 128.f + 6.f / 256.f;  // codes 256-279: 7 bits, 280-287: 8
+    __syncwarp();
     return ok ? kOk : kBadDeflate;
   }
   // dynamic header (RFC 1951 3.2.7)
@@ -353,6 +368,16 @@ __device__ int32_t read_tables(BitReader& br, uint32_t btype, Tables<LB>* T, uin
   __syncwarp();
   if (br.overrun()) return br.wpos > trunc_words ? kTruncated : kOvershoot;
   if (!ok || T->lens[256] == 0) return kBadDeflate;
+  // the code space of the length codes (257 .. nlen-1): a literal-heavy
+  // block has little (the block decoder is chosen by it)
+  {
+    const int sym = 257 + lane;
+    const uint32_t L = sym < nlen ? T->lens[sym] : 0u;
+    float w = L ? __uint_as_float((127u - L) << 23) : 0.f;  // 2^-L
+#pragma unroll
+    for (int d = 16; d; d >>= 1) w += __shfl_xor_sync(0xFFFFFFFFu, w, d);
+    if (lane == 0) T->p_len = w;
+  }
   // the dist lengths must not alias the precode area: move them to 288+
   uint8_t dl = lane < ndist ? T->lens[nlen + lane] : 0;
   __syncwarp();
@@ -708,6 +733,323 @@ __device__ __forceinline__ int32_t huff_block_parallel(
         int32_t ref = -1;
         if (act && ((iL >> 6) & 3) == kKindLen) {
           const int32_t rel = (int32_t)e - (int32_t)dL;  // source, relative to the step start
+          if (rel >= (int32_t)e0) {
+            ref = rel - (int32_t)e0;
+          } else if ((int64_t)o + rel >= 0) {
+            v = *page_addr(ph, orel + rel);
+          } else {
+            v = zero_window ? 0u : (uint32_t)((int64_t)(kMarkerBase + kWindow) + (int64_t)o + rel);
+          }
+        }
+        while (__any_sync(0xFFFFFFFFu, ref >= 0)) {
+          const uint32_t rv = __shfl_sync(0xFFFFFFFFu, v, ref & 31);
+          const int32_t rr = __shfl_sync(0xFFFFFFFFu, ref, ref & 31);
+          if (ref >= 0) {
+            v = rv;
+            ref = rr;
+          }
+        }
+        if (act) *page_addr(ph, orel + (int32_t)e) = (uint16_t)v;
+        if (!zero_window) {
+          const uint32_t m = __ballot_sync(0xFFFFFFFFu, act && v >= kMarkerBase);
+          if (m) marker_end = o + e0 + 32 - __clz(m);
+        }
+        __syncwarp();
+      }
+    }
+    __syncwarp();
+    o += acc;
+    pos += p;
+    if (at_sync) {
+      synced = true;
+      break;
+    }
+    if (eob) break;
+    // the successor's start went by mid-block: it can never be handed over
+    if (kSync && passed_bit < pos) {
+      passed = true;
+      break;
+    }
+  }
+  br.seek(pos, lane);
+  br.refill(lane);
+  ph_io = ph;
+  o_io = o;
+  guard_io = guard;
+  marker_end_io = marker_end;
+  return status;
+}
+
+// ---------------------------------------------------------------------------
+// Huffman block body, lane-parallel over 64-bit steps (page history).
+//
+// A step covers the symbols that start in the next 64 bits.  Lane i looks
+// up the literal/length code at bits i and i + 32 of the step in the LUT
+// only: a literal's successor is its start plus its code length, kept in a
+// 64-entry shared table.  A walk from bit 0 follows literals by one table
+// read each (a broadcast; the loop's only branch); a length code (then its
+// extra bits, distance code and distance extra bits), the end-of-block code,
+// a code longer than the LUT or an invalid code is decoded on the walk by
+// the whole warp from the same bits (shared-memory broadcasts).  Compared
+// with huff_block_parallel, a step carries twice the bits and no lane
+// decodes a distance for a position that is not on the chain, so a literal
+// costs about half the instructions.  Literals go to their output offsets
+// in parallel; matches are copied in passes of 32 entries, sources inside
+// a pass by pointer jumping.
+// ---------------------------------------------------------------------------
+constexpr uint32_t kWideMaxOut = 32 * 258 + 64;  // output bound of one step (>= 2 bits per match)
+// adaptive choice: blocks whose length codes take less of the code space
+// than this decode in 64-bit steps, the others (many matches) in 32-bit steps
+constexpr float kWideMaxLenSpace = 0.3f;
+
+template <int LB, bool kSync>
+__device__ __forceinline__ int32_t huff_block_wide(
+    BitReader& br, const Tables<LB>* T, PageHist& ph_io, const PagePool& pool, uint32_t cid,
+    uint32_t gen, uint64_t& o_io, uint64_t& guard_io, uint64_t& marker_end_io, bool zero_window,
+    uint64_t trunc_words, uint64_t sync_target, uint64_t passed_bit, bool& synced, bool& passed,
+    int lane) {
+  constexpr uint32_t LMASK = (1u << LB) - 1;
+  PageHist ph = ph_io;
+  uint64_t o = o_io, guard = guard_io, marker_end = marker_end_io;
+  uint64_t pos = br.pos();
+  int32_t status = kOk;
+  for (;;) {
+    uint32_t rt = 1000;  // the successor's sync start in this step (>= 64: not here)
+    if (kSync && sync_target != kNoStop && sync_target >= pos) {
+      if (sync_target == pos) {
+        synced = true;
+        break;
+      }
+      if (sync_target - pos < 64) rt = (uint32_t)(sync_target - pos);
+    }
+    if (o >= guard) {
+      ph.advance(o);
+      if (!ph.ensure(pool, cid, gen, o + kWideMaxOut, lane)) {
+        status = kPoolExhausted;
+        break;
+      }
+      const uint64_t pe = (ph.s + 1) << 16;  // end of the current page
+      guard = ph.next != kNoPage ? pe : pe - kWideMaxOut;
+    }
+    // the step's 128 bits from the register-staged input words
+    const uint64_t w0 = pos >> 5;
+    if (w0 < br.win_base || w0 + 3 >= br.win_base + 64) {
+      if (w0 >= br.win_base && w0 < br.win_base + 64) {
+        br.win_base += 32;
+        br.win_cur = br.win_next;
+        br.win_next = br.in32[br.win_base + 32 + lane];
+      } else {
+        br.load_windows(w0 & ~31ull, lane);
+      }
+    }
+    if (w0 + 4 > br.limit_words) {
+      status = w0 + 4 > trunc_words ? kTruncated : kOvershoot;
+      break;
+    }
+    uint32_t W[4];
+    {
+      const uint32_t rel = (uint32_t)(w0 - br.win_base);
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        const uint32_t r = rel + k;
+        const uint32_t a = __shfl_sync(0xFFFFFFFFu, br.win_cur, r & 31);
+        const uint32_t b2 = __shfl_sync(0xFFFFFFFFu, br.win_next, r & 31);
+        W[k] = r < 32 ? a : b2;
+      }
+    }
+    const uint32_t sh0 = (uint32_t)(pos & 31);
+    // lane candidates at step bits lane and lane + 32: 32 bits each
+    uint32_t val0, val1;
+    uint8_t* succ = const_cast<uint8_t*>(T->succ);
+    {
+      const uint32_t t = sh0 + lane;  // 0..62
+      const uint32_t wa = t >> 5, bs = t & 31;
+      const uint32_t lo0 = wa ? W[1] : W[0], mid = wa ? W[2] : W[1], hi1 = wa ? W[3] : W[2];
+      const uint32_t x0 = __funnelshift_r(lo0, mid, bs);
+      const uint32_t x1 = __funnelshift_r(mid, hi1, bs);
+      const uint32_t e0 = T->lit_lut[x0 & LMASK], e1 = T->lit_lut[x1 & LMASK];
+      // a literal: its successor (step bit, < 128); anything else: 0xFF
+      // (decoded on the walk by the whole warp)
+      succ[lane] = (uint8_t)(((e0 & 15) && ((e0 >> 8) & 3) == kKindLit) ? lane + (e0 & 15) : 0xFFu);
+      succ[lane + 32] =
+          (uint8_t)(((e1 & 15) && ((e1 >> 8) & 3) == kKindLit) ? lane + 32 + (e1 & 15) : 0xFFu);
+      val0 = e0 >> 16;
+      val1 = e1 >> 16;
+    }
+    __syncwarp();
+    // The walk: chain = the step bits where symbols on the chain from bit 0
+    // start.  Literals are followed through the successor table (one
+    // shared-memory broadcast each, no branch but the loop's); anything
+    // else is decoded by the whole warp, and a match's extra entries
+    // (length - 1) are counted for the lanes after it (corr).
+    uint64_t chain = 0;
+    uint32_t p = 0, corr0 = 0, corr1 = 0, corr = 0, d0 = 0, d1 = 0;
+    bool m0 = false, m1 = false, eob = false, at_sync = false;
+    for (;;) {
+      uint32_t q;
+      for (;;) {
+        if (kSync && p == rt) {  // the walk ends at the successor's sync start
+          at_sync = true;
+          break;
+        }
+        chain |= 1ull << p;
+        q = succ[p];
+        if (q >= 64) break;
+        p = q;
+      }
+      if (at_sync) break;
+      if (q < 0x80u) {  // a literal that ends past the step
+        p = q;
+        at_sync = kSync && p == rt;
+        break;
+      }
+      // the whole symbol at step bit p, the same in every lane
+      const uint32_t b = sh0 + p;  // bit in W, <= 94
+      if (b + 48 > 128) {          // may not fit: the next step starts here
+        chain &= ~(1ull << p);
+        break;
+      }
+      const uint32_t wa = b >> 5, bs = b & 31;
+      const uint64_t lo = wa == 0 ? ((uint64_t)W[1] << 32 | W[0])
+                                  : (wa == 1 ? ((uint64_t)W[2] << 32 | W[1]) : ((uint64_t)W[3] << 32 | W[2]));
+      const uint32_t h32 = wa == 0 ? W[2] : (wa == 1 ? W[3] : 0u);
+      const uint64_t x = bs ? (lo >> bs) | ((uint64_t)h32 << (64 - bs)) : lo;
+      uint32_t dist = 0;
+      const uint32_t ip = decode_symbol_full<LB>(x, T, &dist);
+      const uint32_t kd = (ip >> 6) & 3;
+      if (kd == kKindBad) {
+        status = kBadDeflate;
+        break;
+      }
+      if (kd == kKindEob) {
+        chain &= ~(1ull << p);
+        p += ip & 63;
+        eob = true;
+        break;
+      }
+      const uint32_t acc_here = (uint32_t)__popcll(chain) - 1 + corr;  // entries before it
+      // a back-reference before the start of the 32 KiB window is invalid
+      if (kd == kKindLen && (uint64_t)dist > o + acc_here + kWindow) {
+        status = kBadDeflate;
+        break;
+      }
+      if (lane == (int)(p & 31)) {
+        if (p >> 5) {
+          m1 = kd == kKindLen; val1 = ip >> 16; d1 = dist;
+        } else {
+          m0 = kd == kKindLen; val0 = ip >> 16; d0 = dist;
+        }
+      }
+      if (kd == kKindLen) {
+        const uint32_t more = (ip >> 16) - 1;
+        corr += more;
+        corr0 += p < (uint32_t)lane ? more : 0u;
+        corr1 += p < (uint32_t)lane + 32 ? more : 0u;
+      }
+      p += ip & 63;
+      if (kSync && p == rt) {
+        at_sync = true;
+        break;
+      }
+      if (p >= 64) break;
+    }
+    if (status != kOk) break;
+    const uint32_t acc = (uint32_t)__popcll(chain) + corr;
+    const bool on0 = (chain >> lane) & 1, on1 = (chain >> (lane + 32)) & 1;
+    const uint32_t ex0 = (uint32_t)__popcll(chain & ((1ull << lane) - 1)) + corr0;
+    const uint32_t ex1 = (uint32_t)__popcll(chain & ((1ull << (lane + 32)) - 1)) + corr1;
+    const int32_t orel = (int32_t)(o - (ph.s << 16));  // o within page seq s
+    if (!__any_sync(0xFFFFFFFFu, m0 || m1)) {
+      // literals only: one store each, at their offsets
+      if (on0) *page_addr(ph, orel + (int32_t)ex0) = (uint16_t)val0;
+      if (on1) *page_addr(ph, orel + (int32_t)ex1) = (uint16_t)val1;
+    } else if (acc <= kWideStage) {
+      // The step's entries are built in the warp's shared stage, then go
+      // to the pages in coalesced stores.  Literals first; then the matches
+      // in chain order (slot-0 lanes, then slot-1 lanes).  Every entry of a
+      // match maps to an entry before the match (final in the stage, or
+      // history), so all its loads are in flight together.
+      uint16_t* stage = const_cast<uint16_t*>(T->stage);
+      if (on0 && !m0) stage[ex0] = (uint16_t)val0;
+      if (on1 && !m1) stage[ex1] = (uint16_t)val1;
+      __syncwarp();
+      // an entry before the match: the stage, history, or before the chunk
+      auto older = [&](int32_t src) -> uint32_t {
+        if (src >= 0) return stage[src];
+        if ((int64_t)o + src >= 0) return *page_addr(ph, orel + src);
+        return zero_window ? 0u : (uint32_t)((int64_t)(kMarkerBase + kWindow) + (int64_t)o + src);
+      };
+      uint32_t mm0 = __ballot_sync(0xFFFFFFFFu, on0 && m0), mm1 = __ballot_sync(0xFFFFFFFFu, on1 && m1);
+      while (mm0 | mm1) {
+        const bool hi = mm0 == 0;
+        const int l = __ffs(hi ? mm1 : mm0) - 1;
+        if (hi) mm1 &= mm1 - 1;
+        else mm0 &= mm0 - 1;
+        const uint32_t mex = __shfl_sync(0xFFFFFFFFu, hi ? ex1 : ex0, l);
+        const uint32_t mlen = __shfl_sync(0xFFFFFFFFu, hi ? val1 : val0, l);
+        const uint32_t md = __shfl_sync(0xFFFFFFFFu, hi ? d1 : d0, l);
+        // entry j of the match copies entry mex + j - md; for an overlapping
+        // match (md < mlen) that source may lie inside the match, and
+        // following it back by md at a time lands on mex - md + (j mod md)
+        const bool overlap = md < mlen;
+        for (uint32_t j0 = 0; j0 < mlen; j0 += 128) {
+          uint32_t v[4];
+#pragma unroll
+          for (int k = 0; k < 4; k++) {
+            const uint32_t j = j0 + 32 * k + lane;
+            const uint32_t jj = overlap ? j % md : j;
+            v[k] = j < mlen ? older((int32_t)(mex + jj) - (int32_t)md) : 0u;
+          }
+#pragma unroll
+          for (int k = 0; k < 4; k++) {
+            const uint32_t j = j0 + 32 * k + lane;
+            if (j < mlen) stage[mex + j] = (uint16_t)v[k];
+          }
+        }
+        __syncwarp();
+      }
+      for (uint32_t i0 = 0; i0 < acc; i0 += 32) {
+        const uint32_t i = i0 + lane;
+        const bool act = i < acc;
+        const uint32_t v = act ? stage[i] : 0u;
+        if (act) *page_addr(ph, orel + (int32_t)i) = (uint16_t)v;
+        if (!zero_window) {
+          const uint32_t m = __ballot_sync(0xFFFFFFFFu, act && v >= kMarkerBase);
+          if (m) marker_end = o + i0 + 32 - __clz(m);
+        }
+      }
+    } else {
+      // The step's entries in passes of 32, lane i writing entry e0 + i: a
+      // literal's value, or a match entry copied from `dist` entries back.
+      // A symbol is named by (slot << 5) | lane; smap holds the one that
+      // starts at each entry of the pass.
+      uint8_t* smap = const_cast<uint8_t*>(T->smap);
+      // packed per slot: value, bit 16 = match
+      const uint32_t q0 = val0 | (m0 ? 0x10000u : 0u), q1 = val1 | (m1 ? 0x10000u : 0u);
+      const uint32_t n0 = on0 ? (m0 ? val0 : 1u) : 0u, n1 = on1 ? (m1 ? val1 : 1u) : 0u;
+      uint32_t carry = 0;  // symbol covering the pass's first entry
+      for (uint32_t e0 = 0; e0 < acc; e0 += 32) {
+        const bool s0 = n0 && ex0 >= e0 && ex0 < e0 + 32;
+        const bool s1 = n1 && ex1 >= e0 && ex1 < e0 + 32;
+        const uint32_t smask = __reduce_or_sync(
+            0xFFFFFFFFu, (s0 ? 1u << (ex0 - e0) : 0u) | (s1 ? 1u << (ex1 - e0) : 0u));
+        if (s0) smap[ex0 - e0] = (uint8_t)lane;
+        if (s1) smap[ex1 - e0] = (uint8_t)(32 + lane);
+        __syncwarp();
+        const uint32_t below = smask & (0xFFFFFFFFu >> (31 - lane));
+        const uint32_t S = below ? smap[31 - __clz(below)] : carry;
+        carry = __shfl_sync(0xFFFFFFFFu, S, 31);
+        const uint32_t qa = __shfl_sync(0xFFFFFFFFu, q0, (int)(S & 31));
+        const uint32_t qb = __shfl_sync(0xFFFFFFFFu, q1, (int)(S & 31));
+        const uint32_t da = __shfl_sync(0xFFFFFFFFu, d0, (int)(S & 31));
+        const uint32_t db = __shfl_sync(0xFFFFFFFFu, d1, (int)(S & 31));
+        const uint32_t qS = S >> 5 ? qb : qa, dS = S >> 5 ? db : da;
+        const uint32_t e = e0 + lane;
+        const bool act = e < acc;
+        uint32_t v = qS & 0xFFFFu;  // a literal's value
+        int32_t ref = -1;
+        if (act && (qS >> 16)) {
+          const int32_t rel = (int32_t)e - (int32_t)dS;  // source, relative to the step start
           if (rel >= (int32_t)e0) {
             ref = rel - (int32_t)e0;
           } else if ((int64_t)o + rel >= 0) {
@@ -1201,14 +1543,18 @@ __device__ int32_t decode_chunk(const uint8_t* __restrict__ in, ChunkDesc d,
             passed_bit = ((const volatile ChunkDesc*)(descs + d.next))->start_bit;
         }
         bool passed = false;
-        status = pool.serial
-                     ? huff_block_serial<LB, kSync>(br, T, ph, pool, cid, gen, o, guard, marker_end,
-                                                    zero_window, trunc_words, sync_target,
-                                                    passed_bit, synced, passed, lane)
-                     : huff_block_parallel<LB, kSync>(br, T, ph, pool, cid, gen, o, guard,
-                                                      marker_end, zero_window, trunc_words,
-                                                      sync_target, passed_bit, synced, passed,
-                                                      lane);
+        if (pool.serial == 1)
+          status = huff_block_serial<LB, kSync>(br, T, ph, pool, cid, gen, o, guard, marker_end,
+                                                zero_window, trunc_words, sync_target, passed_bit,
+                                                synced, passed, lane);
+        else if (pool.serial == 2 || (pool.serial == 3 && T->p_len < kWideMaxLenSpace))
+          status = huff_block_wide<LB, kSync>(br, T, ph, pool, cid, gen, o, guard, marker_end,
+                                              zero_window, trunc_words, sync_target, passed_bit,
+                                              synced, passed, lane);
+        else
+          status = huff_block_parallel<LB, kSync>(br, T, ph, pool, cid, gen, o, guard, marker_end,
+                                                  zero_window, trunc_words, sync_target, passed_bit,
+                                                  synced, passed, lane);
         if (status != kOk || synced) break;
         if (passed) {
           extend(descs[d.next].next);

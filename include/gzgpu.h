@@ -72,9 +72,13 @@ typedef struct {
                          contexts' streams (running blocks are not preempted) */
   int work_order;     /* order in which the persistent decoder takes chunks: 0 = longest
                          expected decode first (default), 1 = in stream order */
-  int decoder;        /* Huffman block bodies: 0 = default, 1 = lane-parallel steps (each
-                         lane decodes a candidate symbol at one bit offset), 2 = warp-uniform
-                         serial decode */
+  int decoder;        /* Huffman block bodies: 0 = default (4), 1 = lane-parallel 32-bit steps
+                         (each lane decodes a whole candidate symbol at one bit offset),
+                         2 = warp-uniform serial decode, 3 = lane-parallel 64-bit steps (each
+                         lane looks up literal codes at two bit offsets; length, end and
+                         long codes are decoded on the chain walk by the whole warp),
+                         4 = chosen per block: 3 where length codes take under 0.3 of the
+                         code space (literal-heavy data), else 1 */
 } gzgpu_config;
 
 typedef struct {

@@ -22,9 +22,10 @@ def G():
     return G
 
 
-# the two Huffman block decoders: lane-parallel steps and warp-uniform serial
-DECODERS = [1, 2]
-DECODER_IDS = ["steps", "serial"]
+# the Huffman block decoders: lane-parallel 32-bit steps, warp-uniform
+# serial, lane-parallel 64-bit steps, chosen per block
+DECODERS = [1, 2, 3, 4]
+DECODER_IDS = ["steps", "serial", "wide", "adaptive"]
 
 
 @pytest.fixture(scope="module", params=DECODERS, ids=DECODER_IDS)
@@ -35,8 +36,8 @@ def ctx(G, request):
 
 
 # history layouts x decoders: (ring_history, decoder)
-LAYOUTS = [(False, 1), (False, 2), (True, 0)]
-LAYOUT_IDS = ["pages-steps", "pages-serial", "ring"]
+LAYOUTS = [(False, 1), (False, 2), (False, 3), (False, 4), (True, 0)]
+LAYOUT_IDS = ["pages-steps", "pages-serial", "pages-wide", "pages-adaptive", "ring"]
 
 
 def _stream(ctype, level, n, seed=1):
