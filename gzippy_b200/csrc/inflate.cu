@@ -822,29 +822,32 @@ __device__ __forceinline__ int32_t huff_block_wide(
       }
       if (sync_target - pos < 64) rt = (uint32_t)(sync_target - pos);
     }
-    if (o >= guard) {
-      ph.advance(o);
-      if (!ph.ensure(pool, cid, gen, o + kWideMaxOut, lane)) {
-        status = kPoolExhausted;
+    // the step's 128 bits come from the register-staged input words; page,
+    // window and limit checks share one branch in the common case
+    const uint64_t w0 = pos >> 5;
+    if (o >= guard || w0 - br.win_base > 60 || w0 + 4 > br.limit_words) {
+      if (o >= guard) {
+        ph.advance(o);
+        if (!ph.ensure(pool, cid, gen, o + kWideMaxOut, lane)) {
+          status = kPoolExhausted;
+          break;
+        }
+        const uint64_t pe = (ph.s + 1) << 16;  // end of the current page
+        guard = ph.next != kNoPage ? pe : pe - kWideMaxOut;
+      }
+      if (w0 < br.win_base || w0 + 3 >= br.win_base + 64) {
+        if (w0 >= br.win_base && w0 < br.win_base + 64) {
+          br.win_base += 32;
+          br.win_cur = br.win_next;
+          br.win_next = br.in32[br.win_base + 32 + lane];
+        } else {
+          br.load_windows(w0 & ~31ull, lane);
+        }
+      }
+      if (w0 + 4 > br.limit_words) {
+        status = w0 + 4 > trunc_words ? kTruncated : kOvershoot;
         break;
       }
-      const uint64_t pe = (ph.s + 1) << 16;  // end of the current page
-      guard = ph.next != kNoPage ? pe : pe - kWideMaxOut;
-    }
-    // the step's 128 bits from the register-staged input words
-    const uint64_t w0 = pos >> 5;
-    if (w0 < br.win_base || w0 + 3 >= br.win_base + 64) {
-      if (w0 >= br.win_base && w0 < br.win_base + 64) {
-        br.win_base += 32;
-        br.win_cur = br.win_next;
-        br.win_next = br.in32[br.win_base + 32 + lane];
-      } else {
-        br.load_windows(w0 & ~31ull, lane);
-      }
-    }
-    if (w0 + 4 > br.limit_words) {
-      status = w0 + 4 > trunc_words ? kTruncated : kOvershoot;
-      break;
     }
     uint32_t W[4];
     {
@@ -884,7 +887,7 @@ __device__ __forceinline__ int32_t huff_block_wide(
     // (length - 1) are counted for the lanes after it (corr).
     uint64_t chain = 0;
     uint32_t p = 0, corr0 = 0, corr1 = 0, corr = 0, d0 = 0, d1 = 0;
-    bool m0 = false, m1 = false, eob = false, at_sync = false;
+    bool m0 = false, m1 = false, any_m = false, eob = false, at_sync = false;
     for (;;) {
       uint32_t q;
       for (;;) {
@@ -941,6 +944,7 @@ __device__ __forceinline__ int32_t huff_block_wide(
         }
       }
       if (kd == kKindLen) {
+        any_m = true;
         const uint32_t more = (ip >> 16) - 1;
         corr += more;
         corr0 += p < (uint32_t)lane ? more : 0u;
@@ -954,15 +958,27 @@ __device__ __forceinline__ int32_t huff_block_wide(
       if (p >= 64) break;
     }
     if (status != kOk) break;
-    const uint32_t acc = (uint32_t)__popcll(chain) + corr;
-    const bool on0 = (chain >> lane) & 1, on1 = (chain >> (lane + 32)) & 1;
-    const uint32_t ex0 = (uint32_t)__popcll(chain & ((1ull << lane) - 1)) + corr0;
-    const uint32_t ex1 = (uint32_t)__popcll(chain & ((1ull << (lane + 32)) - 1)) + corr1;
+    // output offsets: symbols on the chain before the lane's bit, plus the
+    // extra entries of the matches before it (the chain's two halves are
+    // the two slots)
+    const uint32_t c_lo = (uint32_t)chain, c_hi = (uint32_t)(chain >> 32);
+    const uint32_t lt = (1u << lane) - 1;
+    const uint32_t n_lo = __popc(c_lo);
+    const uint32_t acc = n_lo + __popc(c_hi) + corr;
+    const bool on0 = (c_lo >> lane) & 1, on1 = (c_hi >> lane) & 1;
+    const uint32_t ex0 = __popc(c_lo & lt) + corr0;
+    const uint32_t ex1 = n_lo + __popc(c_hi & lt) + corr1;
     const int32_t orel = (int32_t)(o - (ph.s << 16));  // o within page seq s
-    if (!__any_sync(0xFFFFFFFFu, m0 || m1)) {
+    if (!any_m) {
       // literals only: one store each, at their offsets
-      if (on0) *page_addr(ph, orel + (int32_t)ex0) = (uint16_t)val0;
-      if (on1) *page_addr(ph, orel + (int32_t)ex1) = (uint16_t)val1;
+      if (orel + acc <= kPageEntries) {  // the step's entries lie in the current page
+        uint16_t* base = ph.data + (size_t)ph.cur * kPageEntries + orel;
+        if (on0) base[ex0] = (uint16_t)val0;
+        if (on1) base[ex1] = (uint16_t)val1;
+      } else {
+        if (on0) *page_addr(ph, orel + (int32_t)ex0) = (uint16_t)val0;
+        if (on1) *page_addr(ph, orel + (int32_t)ex1) = (uint16_t)val1;
+      }
     } else if (acc <= kWideStage) {
       // The step's entries are built in the warp's shared stage, then go
       // to the pages in coalesced stores.  Literals first; then the matches
