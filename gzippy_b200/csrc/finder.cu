@@ -17,7 +17,7 @@ namespace gzgpu {
 // as soon as a lower window has a hit, so the work is about the distance to
 // the first candidate, split over the CTA's warps.  Stored candidates must
 // also pass start_ok (a stored or dynamic block right after them).
-constexpr int kFinderWarps = 8;
+constexpr int kFinderWarps = 4;
 constexpr uint64_t kFinderWindow = 1024 * kFindGroup;  // bits a warp takes at a time
 
 // Stored block starts, searched first for every speculative chunk: the first

@@ -96,6 +96,7 @@ struct alignas(16) Tables {
     struct {                       // 64-bit steps (huff_block_wide only)
       uint16_t stage[kWideStage];  // the entries of a step with matches
       uint8_t succ[64];            // a literal's successor bit per step bit (0xFF: other)
+      uint16_t succ2[64];          // succ, and in the high byte the successor's succ (0xFF: none)
     };
   };
   uint8_t smap[32];  // output pass: lane of the symbol starting at each entry
@@ -864,6 +865,7 @@ __device__ __forceinline__ int32_t huff_block_wide(
     // lane candidates at step bits lane and lane + 32: 32 bits each
     uint32_t val0, val1;
     uint8_t* succ = const_cast<uint8_t*>(T->succ);
+    uint16_t* succ2 = const_cast<uint16_t*>(T->succ2);
     {
       const uint32_t t = sh0 + lane;  // 0..62
       const uint32_t wa = t >> 5, bs = t & 31;
@@ -873,11 +875,17 @@ __device__ __forceinline__ int32_t huff_block_wide(
       const uint32_t e0 = T->lit_lut[x0 & LMASK], e1 = T->lit_lut[x1 & LMASK];
       // a literal: its successor (step bit, < 128); anything else: 0xFF
       // (decoded on the walk by the whole warp)
-      succ[lane] = (uint8_t)(((e0 & 15) && ((e0 >> 8) & 3) == kKindLit) ? lane + (e0 & 15) : 0xFFu);
-      succ[lane + 32] =
-          (uint8_t)(((e1 & 15) && ((e1 >> 8) & 3) == kKindLit) ? lane + 32 + (e1 & 15) : 0xFFu);
+      const uint32_t a0 = ((e0 & 15) && ((e0 >> 8) & 3) == kKindLit) ? lane + (e0 & 15) : 0xFFu;
+      const uint32_t a1 = ((e1 & 15) && ((e1 >> 8) & 3) == kKindLit) ? lane + 32 + (e1 & 15) : 0xFFu;
+      succ[lane] = (uint8_t)a0;
+      succ[lane + 32] = (uint8_t)a1;
       val0 = e0 >> 16;
       val1 = e1 >> 16;
+      __syncwarp();
+      // two hops: the walk takes two literals per table read
+      const uint32_t b0 = a0 < 64 ? succ[a0] : 0xFFu, b1 = a1 < 64 ? succ[a1] : 0xFFu;
+      succ2[lane] = (uint16_t)(a0 | b0 << 8);
+      succ2[lane + 32] = (uint16_t)(a1 | b1 << 8);
     }
     __syncwarp();
     // The walk: chain = the step bits where symbols on the chain from bit 0
@@ -895,10 +903,25 @@ __device__ __forceinline__ int32_t huff_block_wide(
           at_sync = true;
           break;
         }
-        chain |= 1ull << p;
-        q = succ[p];
-        if (q >= 64) break;
-        p = q;
+        // a = the literal at p's successor, b = a's (0xFF when a is not a
+        // literal inside the step); one branch per two literals
+        const uint32_t v = succ2[p], a = v & 0xFFu, b = v >> 8;
+        if (b >= 64 || (kSync && a == rt)) {
+          chain |= 1ull << p;
+          if (a >= 64) {
+            q = a;
+          } else if (kSync && a == rt) {
+            p = a;
+            at_sync = true;
+          } else {
+            chain |= 1ull << a;
+            p = a;
+            q = b;
+          }
+          break;
+        }
+        chain |= (1ull << p) | (1ull << a);
+        p = b;
       }
       if (at_sync) break;
       if (q < 0x80u) {  // a literal that ends past the step
