@@ -17,7 +17,7 @@ namespace gzgpu {
 // as soon as a lower window has a hit, so the work is about the distance to
 // the first candidate, split over the CTA's warps.  Stored candidates must
 // also pass start_ok (a stored or dynamic block right after them).
-constexpr int kFinderWarps = 4;
+constexpr int kFinderWarps = 2;
 constexpr uint64_t kFinderWindow = 1024 * kFindGroup;  // bits a warp takes at a time
 
 // Stored block starts, searched first for every speculative chunk: the first
@@ -80,18 +80,35 @@ __global__ void __launch_bounds__(kStoredThreads)
   }
 }
 
+// The precode leaf count of 4 code-length codes (12 bits) for every value,
+// built at compile time and read through the L1 cache: a CTA needs no
+// shared copy, so more small CTAs fit on an SM.
+struct LeafLut {
+  uint16_t v[4096];
+  constexpr LeafLut() : v() {
+    for (int i = 0; i < 4096; i++) {
+      uint32_t sum = 0;
+      for (int k = 0; k < 4; k++) {
+        const uint32_t L = (i >> (3 * k)) & 7;
+        sum += L ? 1u << (7 - L) : 0u;
+      }
+      v[i] = (uint16_t)sum;
+    }
+  }
+};
+__device__ const LeafLut d_leaf_lut = LeafLut();
+
 __global__ void __launch_bounds__(32 * kFinderWarps)
     finder_kernel(const uint8_t* __restrict__ in, ChunkDesc* descs,
                   const uint32_t* __restrict__ spec, uint32_t n_spec) {
   __shared__ unsigned long long best_win;
   __shared__ uint64_t hit_lo[kFinderWarps], hit_hi[kFinderWarps], hit_win[kFinderWarps];
-  __shared__ uint16_t leaf_lut[4096];
   __shared__ FinderLists lists[kFinderWarps];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   if (blockIdx.x >= n_spec) return;
   ChunkDesc& d = descs[spec[blockIdx.x]];
   if (d.flags & kChunkValid) return;  // a stored or sync start was found first
-  for (int i = threadIdx.x; i < 4096; i += blockDim.x) leaf_lut[i] = (uint16_t)precode_leaves4(i);
+  const uint16_t* leaf_lut = d_leaf_lut.v;
   const uint64_t from = d.guess_bit, to = d.limit_bit, nbytes = d.in_end;
   if (threadIdx.x == 0) best_win = ~0ull;
   if (lane == 0) hit_win[warp] = ~0ull;
