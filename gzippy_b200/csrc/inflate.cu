@@ -787,16 +787,20 @@ __device__ __forceinline__ int32_t huff_block_parallel(
 // A step covers the symbols that start in the next 64 bits.  Lane i looks
 // up the literal/length code at bits i and i + 32 of the step in the LUT
 // only: a literal's successor is its start plus its code length, kept in a
-// 64-entry shared table.  A walk from bit 0 follows literals by one table
-// read each (a broadcast; the loop's only branch); a length code (then its
-// extra bits, distance code and distance extra bits), the end-of-block code,
-// a code longer than the LUT or an invalid code is decoded on the walk by
-// the whole warp from the same bits (shared-memory broadcasts).  Compared
-// with huff_block_parallel, a step carries twice the bits and no lane
-// decodes a distance for a position that is not on the chain, so a literal
-// costs about half the instructions.  Literals go to their output offsets
-// in parallel; matches are copied in passes of 32 entries, sources inside
-// a pass by pointer jumping.
+// 64-entry shared table beside a second one holding each entry's
+// successor's successor.  A walk from bit 0 follows literals two at a time
+// through that table (one broadcast read and one branch per two literals);
+// a length code (then its extra bits, distance code and distance extra
+// bits), the end-of-block code, a code longer than the LUT or an invalid
+// code is decoded on the walk by the whole warp from the same bits
+// (shared-memory broadcasts).  Compared with huff_block_parallel, a step
+// carries twice the bits and no lane decodes a distance for a position that
+// is not on the chain.  The chain is a 64-bit mask of symbol starts, so each
+// lane's output offset is a population count.  Literals go to their output
+// offsets in parallel; a step with matches builds its entries in a shared
+// stage, where every match entry maps to an entry before the match, and
+// writes them out in coalesced stores (larger steps copy in passes of 32
+// entries, sources inside a pass by pointer jumping).
 // ---------------------------------------------------------------------------
 constexpr uint32_t kWideMaxOut = 32 * 258 + 64;  // output bound of one step (>= 2 bits per match)
 // adaptive choice: blocks whose length codes take less of the code space
