@@ -1386,7 +1386,7 @@ namespace {
 // kStageSlot slots, allocated once), gathered and scattered by up to
 // kCopyThreads host threads while the other slot's DMA runs.
 constexpr size_t kDirectBytes = 1u << 20;
-constexpr int kCopyThreads = 8;
+constexpr int kCopyThreads = 16;
 
 bool host_pinned(const void* p) {
   cudaPointerAttributes a;
@@ -1406,7 +1406,7 @@ struct CopyJob {
 void parallel_copy(const std::vector<CopyJob>& jobs) {
   size_t total = 0;
   for (const CopyJob& j : jobs) total += j.len;
-  int nt = (int)std::min<size_t>(kCopyThreads, total / (8u << 20) + 1);
+  int nt = (int)std::min<size_t>(kCopyThreads, total / (2u << 20) + 1);
   nt = std::max(1, std::min(nt, (int)std::thread::hardware_concurrency()));
   if (nt <= 1) {
     for (const CopyJob& j : jobs) memcpy(j.dst, j.src, j.len);
