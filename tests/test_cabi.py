@@ -55,3 +55,35 @@ def test_not_gzip_is_empty_without_device_work():
     buf = (ctypes.c_uint8 * 4)()
     rc = lib.gzgpu_decompress(ctypes.c_void_p(1), b"abc", 3, buf, 4, ctypes.byref(n))
     assert rc == G.NOT_GZIP and n.value == 0
+
+
+def _c_config_layout(tmp_path):
+    """(sizeof, [(field, offset)]) of gzgpu_config, from the C compiler."""
+    import subprocess
+    src = open(HEADER).read()
+    block = re.search(r"typedef struct \{(.*?)\} gzgpu_config;", src, flags=re.S).group(1)
+    block = re.sub(r"/\*.*?\*/", "", block, flags=re.S)
+    fields = re.findall(r"\b([a-z_]+)\s*;", block)
+    prog = tmp_path / "layout.c"
+    lines = ['#include <stddef.h>', '#include <stdio.h>', f'#include "{HEADER}"', "int main(void) {",
+             '  printf("%zu\\n", sizeof(gzgpu_config));']
+    lines += [f'  printf("{f} %zu\\n", offsetof(gzgpu_config, {f}));' for f in fields]
+    lines += ["  return 0;", "}"]
+    prog.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.check_call(["gcc", "-std=c99", "-o", str(exe), str(prog)])
+    out = subprocess.check_output([str(exe)], text=True).split("\n")
+    return int(out[0]), [(ln.split()[0], int(ln.split()[1])) for ln in out[1:] if ln]
+
+
+def test_config_layout_matches_bindings(tmp_path):
+    """The Python binding's Config and the Rust shim's GzgpuConfig in
+    INTEGRATION.md list gzgpu_config's fields in the header's order, and the
+    Python layout has the C compiler's offsets and size."""
+    import gzippy_b200 as G
+    size, fields = _c_config_layout(tmp_path)
+    assert ctypes.sizeof(G.Config) == size
+    assert [(n, getattr(G.Config, n).offset) for n, _ in G.Config._fields_] == fields
+    doc = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    rust = re.search(r"pub struct GzgpuConfig \{(.*?)\}", doc, flags=re.S).group(1)
+    assert re.findall(r"pub ([a-z_]+):", rust) == [n for n, _ in fields]
