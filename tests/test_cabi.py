@@ -57,20 +57,24 @@ def test_not_gzip_is_empty_without_device_work():
     assert rc == G.NOT_GZIP and n.value == 0
 
 
-def _c_config_layout(tmp_path):
-    """(sizeof, [(field, offset)]) of gzgpu_config, from the C compiler."""
+def _c_layout(tmp_path, name):
+    """(sizeof, [(field, offset)]) of the header's struct `name`, from the C
+    compiler."""
     import subprocess
     src = open(HEADER).read()
-    block = re.search(r"typedef struct \{(.*?)\} gzgpu_config;", src, flags=re.S).group(1)
+    block = re.search(r"typedef struct \{([^{}]*?)\} " + name + ";", src, flags=re.S).group(1)
     block = re.sub(r"/\*.*?\*/", "", block, flags=re.S)
-    fields = re.findall(r"\b([a-z_]+)\s*;", block)
-    prog = tmp_path / "layout.c"
+    fields = []
+    for decl in block.split(";"):
+        parts = [x.strip() for x in decl.split(",") if x.strip()]
+        fields += [x.split()[-1].lstrip("*") for x in parts]
+    prog = tmp_path / (name + ".c")
     lines = ['#include <stddef.h>', '#include <stdio.h>', f'#include "{HEADER}"', "int main(void) {",
-             '  printf("%zu\\n", sizeof(gzgpu_config));']
-    lines += [f'  printf("{f} %zu\\n", offsetof(gzgpu_config, {f}));' for f in fields]
+             f'  printf("%zu\\n", sizeof({name}));']
+    lines += [f'  printf("{f} %zu\\n", offsetof({name}, {f}));' for f in fields]
     lines += ["  return 0;", "}"]
     prog.write_text("\n".join(lines) + "\n")
-    exe = tmp_path / "layout"
+    exe = tmp_path / name
     subprocess.check_call(["gcc", "-std=c99", "-o", str(exe), str(prog)])
     out = subprocess.check_output([str(exe)], text=True).split("\n")
     return int(out[0]), [(ln.split()[0], int(ln.split()[1])) for ln in out[1:] if ln]
@@ -81,9 +85,23 @@ def test_config_layout_matches_bindings(tmp_path):
     INTEGRATION.md list gzgpu_config's fields in the header's order, and the
     Python layout has the C compiler's offsets and size."""
     import gzippy_b200 as G
-    size, fields = _c_config_layout(tmp_path)
+    size, fields = _c_layout(tmp_path, "gzgpu_config")
     assert ctypes.sizeof(G.Config) == size
     assert [(n, getattr(G.Config, n).offset) for n, _ in G.Config._fields_] == fields
     doc = open(os.path.join(ROOT, "INTEGRATION.md")).read()
     rust = re.search(r"pub struct GzgpuConfig \{(.*?)\}", doc, flags=re.S).group(1)
     assert re.findall(r"pub ([a-z_]+):", rust) == [n for n, _ in fields]
+
+
+@pytest.mark.parametrize("c_name,py_name", [
+    ("gzgpu_span", "Span"), ("gzgpu_out", "Out"), ("gzgpu_stats", "Stats"),
+    ("gzgpu_server_config", "ServerConfig"), ("gzgpu_request_times", "RequestTimes"),
+    ("gzgpu_server_stats", "ServerStats")])
+def test_struct_layouts_match_bindings(tmp_path, c_name, py_name):
+    """Every other struct of the C ABI has the Python binding's field order,
+    offsets and size."""
+    import gzippy_b200 as G
+    cls = getattr(G, py_name)
+    size, fields = _c_layout(tmp_path, c_name)
+    assert ctypes.sizeof(cls) == size
+    assert [(n, getattr(cls, n).offset) for n, _ in cls._fields_] == fields
