@@ -302,12 +302,13 @@ constexpr uint64_t kMinPartitionBits = 8ull << 13;
 constexpr uint64_t kMinPieceBits = 4ull << 13;
 
 static uint64_t pick_chunk_bytes(uint64_t in_len) {
-  // about five chunks per decoding warp on large inputs, which the
+  // several chunks per decoding warp on large inputs, which the
   // longest-first order balances; smaller chunks for small inputs so the
-  // warps still fill (measured on the 1 GiB mixed stream, whole decode:
-  // 64 KiB 45.0 ms, 48 KiB 45.1, 32 KiB 43.2, 24 KiB 45.3; below 32 KiB the
-  // finder and the per-chunk resolve work outgrow the shorter tail)
-  uint64_t c = 32 << 10;
+  // warps still fill.  Measured on the 1 GiB mixed stream, whole decode,
+  // one box: 48 KiB 43.5 ms, 40 KiB 44.1, 32 KiB 36.4-38.6, 24 KiB 35.3
+  // (the decode's tail shrinks faster than the finder and the per-chunk
+  // resolve work grow)
+  uint64_t c = 24 << 10;
   if (in_len < (4ull << 20)) c = 16 << 10;
   return c;
 }
